@@ -1,0 +1,269 @@
+/* vajra_pdhg.h -- C ABI of the B200 (sm_100a) restarted-PDHG LP backend.
+ *
+ * The library (libvajra_pdhg.so) replaces the reference's src/solvers/gpu/ backend:
+ * gpu_context.cpp (probe + dispatch), pdhg_cuda.cu (host driver) and spmv_kernels.cuh
+ * (device kernels).  All entry points are plain C: POD structs, host or device pointers
+ * with explicit sizes, an int32 status, and no exceptions across the boundary.  A C++20
+ * shim (vajra-opt_b200/shim/indus_gpu_dropin.cpp) maps the reference's C++ surface
+ * indus::gpu::{solve_pdhg_gpu, probe_device, is_cuda_available, get_last_gpu_timing}
+ * (include/indus/gpu.hpp:49-59) onto these functions.
+ *
+ * Conventions (same as the reference Model, include/indus/model.hpp:16-55):
+ *   - A is m x n in CSC: col_ptr[n+1] (int64), row_idx[nnz] (int32, ascending within a
+ *     column, no duplicates), values[nnz] (double).
+ *   - Infinite bounds are +-1e20 (or beyond).
+ *   - row_dual uses the verifier's sign convention (<= row: y <= 0, >= row: y >= 0),
+ *     col_dual = c - A^T row_dual, row_value = A x, objective includes objective_offset.
+ *   - status values are indus::SolveStatus (include/indus/types.hpp:34-47).
+ * There is no CPU fallback: without a usable CUDA device every solve returns
+ * VAJRA_ERR_NO_DEVICE and status UNSUPPORTED.
+ */
+#ifndef VAJRA_PDHG_H
+#define VAJRA_PDHG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t vajra_status;
+enum {
+    VAJRA_OK = 0,
+    VAJRA_ERR_INVALID_ARGUMENT = 1,
+    VAJRA_ERR_NO_DEVICE = 2,
+    VAJRA_ERR_CUDA = 3,
+    VAJRA_ERR_OUT_OF_MEMORY = 4,
+    VAJRA_ERR_WAIT_TIMEOUT = 5,  /* a bounded device-side wait gave up (batched kernel) */
+    VAJRA_ERR_INTERNAL = 6
+};
+
+/* indus::SolveStatus values (include/indus/types.hpp:34-47). */
+enum {
+    VAJRA_SOLVE_NOT_SOLVED = 0,
+    VAJRA_SOLVE_OPTIMAL = 1,
+    VAJRA_SOLVE_UNBOUNDED = 3,
+    VAJRA_SOLVE_FEASIBLE = 5,
+    VAJRA_SOLVE_ITERATION_LIMIT = 6,
+    VAJRA_SOLVE_TIME_LIMIT = 7,
+    VAJRA_SOLVE_NUMERICAL_ERROR = 9,
+    VAJRA_SOLVE_MODEL_ERROR = 10,
+    VAJRA_SOLVE_UNSUPPORTED = 11
+};
+
+/* Algorithms. */
+enum {
+    /* CpuPdhgSolver::solve semantics (src/solvers/pdhg/pdhg.cpp:70-440) in FP64 on the
+     * device, evaluated in the reference's operation order: Ruiz (10 passes), power-
+     * iteration norm, tau = sigma = 0.95/||A||, checks every check_frequency, tau/sigma
+     * rebalancing, stagnation restart, best-iterate return.  Bit-identical to the
+     * reference CPU solver on the same input. */
+    VAJRA_ALGO_REFERENCE = 0,
+    /* Restarted reflected Halpern PDHG with KKT-based adaptive restarts and primal-weight
+     * updates, terminated on the FP64 relative KKT error of the original problem. */
+    VAJRA_ALGO_HALPERN = 1
+};
+
+/* Precision of VAJRA_ALGO_HALPERN (VAJRA_ALGO_REFERENCE is always FP64). */
+enum {
+    VAJRA_PREC_FP64 = 0,   /* "plain" form: FP64 values, iterates and accumulation       */
+    VAJRA_PREC_MIXED = 1   /* FP32 values/iterates/SpMV accumulation, FP64 KKT, gap,
+                              restart and primal-weight decisions, then an FP64 polish
+                              restarted from the FP32 iterate                            */
+};
+
+/* The reference Model (include/indus/model.hpp:16-55) as CSC host arrays. */
+typedef struct vajra_lp {
+    int32_t num_rows;
+    int32_t num_cols;
+    int64_t nnz;
+    const int64_t* col_ptr;
+    const int32_t* row_idx;
+    const double* values;
+    const double* c;
+    const double* col_lower;
+    const double* col_upper;
+    const double* row_lower;
+    const double* row_upper;
+    int32_t sense;             /* 0 minimise, 1 maximise (ObjSense)                     */
+    double objective_offset;
+} vajra_lp;
+
+/* Solver options: the PDHG keys of indus::Options (include/indus/options.hpp:10-41,
+ * read at src/solvers/pdhg/pdhg.cpp:58-68) plus this backend's own settings. */
+typedef struct vajra_opts {
+    int32_t algorithm;          /* VAJRA_ALGO_*                                          */
+    int32_t precision;          /* VAJRA_PREC_* (HALPERN only)                           */
+    double tolerance;           /* REFERENCE: max-abs primal and dual residual
+                                   ("tolerance"); HALPERN: relative KKT target           */
+    double gap_tolerance;       /* REFERENCE: relative gap ("gap_tolerance")             */
+    double time_limit;          /* seconds (Options::time_limit)                         */
+    int64_t iteration_limit;    /* Options::iteration_limit                              */
+    int32_t check_frequency;    /* REFERENCE: "check_frequency" (100); HALPERN: KKT /
+                                   restart evaluation interval (64)                      */
+    int32_t enable_scaling;     /* Options::enable_scaling                               */
+    int32_t pock_chambolle;     /* HALPERN: 1 = Pock-Chambolle (alpha = 1) after Ruiz     */
+    int32_t ruiz_iterations;    /* 10 (tol::kMaxRuizIterations)                          */
+    double reflection;          /* HALPERN: reflection coefficient of the Halpern step   */
+    double mixed_switch_tolerance; /* MIXED: FP32 phase hands over to FP64 below this
+                                      relative KKT (or when FP32 stalls)                 */
+    int32_t device;             /* CUDA device ordinal                                   */
+    int32_t autotune;           /* 1 = time SpMV variants at set-up and keep the fastest */
+    int32_t verbose;
+    int32_t reserved[7];
+} vajra_opts;
+
+/* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and
+ * col_dual n, row_value and row_dual m. */
+typedef struct vajra_result {
+    double* col_value;
+    double* row_value;
+    double* row_dual;
+    double* col_dual;
+    int32_t status;             /* VAJRA_SOLVE_*                                         */
+    int64_t iterations;
+    double objective_value;
+    double dual_objective;
+    /* PdhgDiagnostics surface (include/indus/pdhg.hpp:30-43) */
+    int32_t restart_count;
+    double primal_residual;
+    double dual_residual;
+    double duality_gap;
+    double spectral_norm_estimate;
+    double tau;
+    double sigma;
+    int32_t converged;
+    /* FP64 relative KKT of the returned point on the original problem */
+    double rel_primal;
+    double rel_dual;
+    double rel_gap;
+    double rel_kkt;
+    double primal_weight;
+    int64_t fp32_iterations;
+    int64_t fp64_iterations;
+    /* GpuTimingDiagnostics surface (include/indus/gpu.hpp:37-46) */
+    double upload_time_sec;
+    double setup_time_sec;
+    double iteration_time_sec;
+    double download_time_sec;
+    double total_time_sec;
+    int64_t host_device_transfers;
+    int32_t spmv_group_a;       /* lanes per row chosen for A x      (0 = sequential)     */
+    int32_t spmv_group_at;      /* lanes per row chosen for A^T y                          */
+    char status_message[256];
+} vajra_result;
+
+/* GpuDeviceInfo (include/indus/gpu.hpp:16-24). */
+typedef struct vajra_device_info {
+    int32_t available;
+    char device_name[256];
+    uint64_t total_vram_bytes;
+    uint64_t free_vram_bytes;
+    int32_t compute_capability_major;
+    int32_t compute_capability_minor;
+    int32_t multi_processor_count;
+} vajra_device_info;
+
+/* GpuTimingDiagnostics (include/indus/gpu.hpp:37-46), per calling thread. */
+typedef struct vajra_timing {
+    double upload_time_sec;
+    double iteration_time_sec;
+    double download_time_sec;
+    double total_time_sec;
+    int64_t host_device_transfers;
+    int64_t iterations;
+    char device_name[256];
+    char kernel_mode[64];
+} vajra_timing;
+
+/* DeviceDiagnostics (include/indus/gpu.hpp:27-34). */
+typedef struct vajra_device_diagnostics {
+    double primal_residual;
+    double dual_residual;
+    double objective;
+    double duality_gap;
+    int32_t converged;
+    int32_t numerical_error;
+} vajra_device_diagnostics;
+
+typedef struct vajra_pdhg vajra_pdhg;  /* opaque: one LP resident on one device */
+
+/* ---- solver ------------------------------------------------------------------ */
+
+/* Fills the defaults (HALPERN, MIXED, tolerance 1e-6, check every 64, ...). */
+void vajra_default_opts(vajra_opts* opts);
+
+/* Replaces indus::gpu::solve_pdhg_gpu (include/indus/gpu.hpp:59;
+ * src/solvers/gpu/gpu_context.cpp:65-80 -> src/solvers/gpu/pdhg_cuda.cu:109-375):
+ * upload, device set-up, iterate, download, all in one call.  Host buffers in and out. */
+vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_result* result);
+
+/* Split form of vajra_pdhg_solve for callers that solve the same LP repeatedly
+ * (pdhg_cuda.cu:187-227 upload once): create uploads the LP to the device; run does the
+ * device set-up and the solve from the resident copy; destroy frees it. */
+vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra_pdhg** handle);
+vajra_status vajra_pdhg_run(vajra_pdhg* handle, vajra_result* result);
+vajra_status vajra_pdhg_destroy(vajra_pdhg* handle);
+
+/* ---- device probe and telemetry ------------------------------------------------ */
+
+/* Replaces indus::gpu::probe_device (gpu.hpp:49; gpu_context.cpp:16-59). */
+vajra_status vajra_probe_device(int32_t device, vajra_device_info* info);
+/* Replaces indus::gpu::is_cuda_available (gpu.hpp:52; gpu_context.cpp:61-63). */
+int32_t vajra_is_cuda_available(void);
+/* Replaces indus::gpu::get_last_gpu_timing (gpu.hpp:55; pdhg_cuda.cu:101-107);
+ * thread-local instead of the reference's process-global g_last_gpu_timing. */
+void vajra_last_timing(vajra_timing* out);
+/* Human-readable text for a vajra_status. */
+const char* vajra_status_string(vajra_status status);
+
+/* ---- kernel-level entry points (device pointers, caller's stream; NULL = default) --
+ * Each mirrors one kernel of src/solvers/gpu/spmv_kernels.cuh; the _f32 forms are the
+ * mixed-precision variants.  Row pointers are int64 as in the reference CSR/CSC. */
+
+/* spmv_csr_warp_kernel (spmv_kernels.cuh:39-76): y = A x over CSR. */
+vajra_status vajra_csr_spmv_f64(int32_t rows, const int64_t* row_ptr, const int32_t* col_idx,
+                                const double* values, const double* x, double* y, void* stream);
+vajra_status vajra_csr_spmv_f32(int32_t rows, const int64_t* row_ptr, const int32_t* col_idx,
+                                const float* values, const float* x, float* y, void* stream);
+/* spmv_csc_transpose_warp_kernel (spmv_kernels.cuh:101-138): v = A^T y over CSC. */
+vajra_status vajra_csc_spmv_transpose_f64(int32_t cols, const int64_t* col_ptr,
+                                          const int32_t* row_idx, const double* values,
+                                          const double* y, double* v, void* stream);
+vajra_status vajra_csc_spmv_transpose_f32(int32_t cols, const int64_t* col_ptr,
+                                          const int32_t* row_idx, const float* values,
+                                          const float* y, float* v, void* stream);
+/* dual_update_kernel (spmv_kernels.cuh:163-180). */
+vajra_status vajra_dual_prox_f64(int32_t rows, double sigma, const double* ax,
+                                 const double* row_lower, const double* row_upper, double* y,
+                                 void* stream);
+/* primal_update_kernel (spmv_kernels.cuh:185-206). */
+vajra_status vajra_primal_prox_f64(int32_t cols, double tau, const double* aty, const double* c,
+                                   const double* col_lower, const double* col_upper, double* x,
+                                   double* x_bar, void* stream);
+/* compute_diagnostics_device_kernel (spmv_kernels.cuh:210-278); out is a device pointer.
+ * Deterministic block reductions instead of the reference's CAS atomics. */
+vajra_status vajra_device_diagnostics_f64(int32_t rows, int32_t cols, const double* ax,
+                                          const double* row_lower, const double* row_upper,
+                                          const double* aty, const double* c, const double* x,
+                                          const double* y, const double* col_lower,
+                                          const double* col_upper,
+                                          vajra_device_diagnostics* out, void* stream);
+/* One fused PDHG iteration (the 4-launch loop body of pdhg_cuda.cu:261-279 as 2 kernels):
+ * w = A x_bar with the dual prox fused into its epilogue, then v = A^T y with the primal
+ * prox and extrapolation fused.  CSR of A and CSC of A (= CSR of A^T). */
+vajra_status vajra_pdhg_step_f64(int32_t rows, int32_t cols,
+                                 const int64_t* row_ptr, const int32_t* col_idx,
+                                 const double* csr_values, const int64_t* col_ptr,
+                                 const int32_t* row_idx, const double* csc_values,
+                                 const double* row_lower, const double* row_upper,
+                                 const double* c, const double* col_lower,
+                                 const double* col_upper, double sigma, double tau,
+                                 double* x, double* x_bar, double* y, double* w, double* v,
+                                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VAJRA_PDHG_H */

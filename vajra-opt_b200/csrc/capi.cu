@@ -1,0 +1,554 @@
+// C ABI of libvajra_pdhg (include/vajra_pdhg.h).  Every entry point returns a status and
+// never lets an exception escape.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace vajra {
+
+namespace {
+thread_local char g_error[512] = "";
+thread_local vajra_timing g_last_timing = {};
+}  // namespace
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+}
+
+const char* last_error() { return g_error; }
+
+vajra_status cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+    set_error("CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), what, file, line);
+    if (e == cudaErrorMemoryAllocation) return VAJRA_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return VAJRA_ERR_NO_DEVICE;
+    return VAJRA_ERR_CUDA;
+}
+
+void copy_out_vector(double* dst, const double* dev, int count, cudaStream_t st) {
+    if (dst && count > 0) cudaMemcpyAsync(dst, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, st);
+}
+
+// Closed forms (no device work): n == 0 and m == 0 follow pdhg.cpp:88-127.
+bool solve_trivial(const vajra_pdhg* h, vajra_result* r) {
+    const int m = h->m, n = h->n;
+    const bool is_max = h->sense != 0;
+    if (n != 0 && m != 0) return false;
+    auto fill = [](double* p, int k) { if (p) for (int i = 0; i < k; ++i) p[i] = 0.0; };
+    fill(r->col_value, n);
+    fill(r->row_value, m);
+    fill(r->row_dual, m);
+    fill(r->col_dual, n);
+    r->iterations = 0;
+    r->converged = 1;
+    r->status = VAJRA_SOLVE_OPTIMAL;
+    if (n == 0) {
+        r->objective_value = h->objective_offset;
+        std::snprintf(r->status_message, sizeof(r->status_message), "no columns: closed form");
+        return true;
+    }
+    double obj = h->objective_offset;
+    for (int j = 0; j < n; ++j) {
+        const double cj = is_max ? -h->h_c[j] : h->h_c[j];
+        const double lj = h->h_cl[j], uj = h->h_cu[j];
+        double xj;
+        if (cj > 1e-7) {
+            if (lj <= -1e20) { r->status = VAJRA_SOLVE_UNBOUNDED; r->converged = 0; break; }
+            xj = lj;
+        } else if (cj < -1e-7) {
+            if (uj >= 1e20) { r->status = VAJRA_SOLVE_UNBOUNDED; r->converged = 0; break; }
+            xj = uj;
+        } else {
+            xj = (lj > 0.0) ? lj : ((uj < 0.0) ? uj : 0.0);
+        }
+        if (r->col_value) r->col_value[j] = xj;
+        if (r->col_dual) r->col_dual[j] = h->h_c[j];
+        obj += h->h_c[j] * xj;
+    }
+    r->objective_value = obj;
+    r->dual_objective = obj;
+    std::snprintf(r->status_message, sizeof(r->status_message), "no rows: closed form");
+    return true;
+}
+
+// Device validation of the index array: every row index in [0, m), ascending within a
+// column.  col_ptr has already been checked on the host, so every access is in bounds.
+__global__ void k_validate_rows(int n, int m, const int64_t* __restrict__ col_ptr,
+                                const int32_t* __restrict__ row_idx, int* __restrict__ bad) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int prev = -1;
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+        const int r = row_idx[k];
+        if (r < 0 || r >= m) { atomicOr(bad, 1); return; }
+        if (r <= prev) { atomicOr(bad, 2); return; }
+        prev = r;
+    }
+}
+
+static vajra_status validate_host(const vajra_lp* lp) {
+    if (!lp) { set_error("lp is NULL"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    const int m = lp->num_rows, n = lp->num_cols;
+    if (m < 0 || n < 0) { set_error("negative dimensions"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    if (!lp->col_ptr || (n > 0 && (!lp->c || !lp->col_lower || !lp->col_upper)) ||
+        (m > 0 && (!lp->row_lower || !lp->row_upper))) {
+        set_error("NULL array in vajra_lp");
+        return VAJRA_ERR_INVALID_ARGUMENT;
+    }
+    if (lp->col_ptr[0] != 0) { set_error("col_ptr[0] != 0"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    for (int j = 0; j < n; ++j)
+        if (lp->col_ptr[j + 1] < lp->col_ptr[j]) { set_error("col_ptr decreases at column %d", j); return VAJRA_ERR_INVALID_ARGUMENT; }
+    if (lp->col_ptr[n] != lp->nnz) { set_error("col_ptr[n] != nnz"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    if (lp->nnz > 0 && (!lp->row_idx || !lp->values)) { set_error("NULL row_idx / values"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    if (lp->nnz > 0 && m == 0) { set_error("nonzeros in a matrix without rows"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    // Model::validate (src/engine/model.cpp:35-150): NaN or crossed bounds are model errors.
+    for (int j = 0; j < n; ++j) {
+        const double l = lp->col_lower[j], u = lp->col_upper[j];
+        if (std::isnan(l) || std::isnan(u) || l > u + 1e-11) { set_error("column %d has NaN or crossed bounds", j); return VAJRA_ERR_INVALID_ARGUMENT; }
+    }
+    for (int i = 0; i < m; ++i) {
+        const double l = lp->row_lower[i], u = lp->row_upper[i];
+        if (std::isnan(l) || std::isnan(u) || l > u + 1e-11) { set_error("row %d has NaN or crossed bounds", i); return VAJRA_ERR_INVALID_ARGUMENT; }
+    }
+    return VAJRA_OK;
+}
+
+static vajra_status validate_device(const vajra_pdhg* h) {
+    if (h->nnz == 0 || h->n == 0) return VAJRA_OK;
+    DeviceBuffer<int> bad;
+    VJ_TRY(bad.alloc(1));
+    VJ_CUDA(cudaMemsetAsync(bad.get(), 0, sizeof(int), h->stream));
+    k_validate_rows<<<grid_for(h->n), kThreads, 0, h->stream>>>(h->n, h->m, h->lp.col_ptr.get(), h->lp.row_idx.get(), bad.get());
+    VJ_LAUNCH_CHECK();
+    int hb = 0;
+    VJ_CUDA(cudaMemcpyAsync(&hb, bad.get(), sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    VJ_CUDA(cudaStreamSynchronize(h->stream));
+    if (hb & 1) { set_error("row index out of range"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    if (hb & 2) { set_error("row indices not strictly ascending within a column (duplicates or unsorted)"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    return VAJRA_OK;
+}
+
+static void fail_result(vajra_result* r, vajra_status s) {
+    if (!r) return;
+    r->status = (s == VAJRA_ERR_NO_DEVICE) ? VAJRA_SOLVE_UNSUPPORTED
+              : (s == VAJRA_ERR_INVALID_ARGUMENT) ? VAJRA_SOLVE_MODEL_ERROR : VAJRA_SOLVE_NUMERICAL_ERROR;
+    std::snprintf(r->status_message, sizeof(r->status_message), "%s: %s", vajra_status_string(s), last_error());
+}
+
+}  // namespace vajra
+
+using namespace vajra;
+
+extern "C" {
+
+const char* vajra_status_string(vajra_status s) {
+    switch (s) {
+        case VAJRA_OK: return "ok";
+        case VAJRA_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case VAJRA_ERR_NO_DEVICE: return "no CUDA device";
+        case VAJRA_ERR_CUDA: return "CUDA error";
+        case VAJRA_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case VAJRA_ERR_WAIT_TIMEOUT: return "device wait timed out";
+        case VAJRA_ERR_INTERNAL: return "internal error";
+        default: return "unknown status";
+    }
+}
+
+void vajra_default_opts(vajra_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->algorithm = VAJRA_ALGO_HALPERN;
+    o->precision = VAJRA_PREC_MIXED;
+    o->tolerance = 1e-6;
+    o->gap_tolerance = 1e-6;
+    o->time_limit = 1e20;
+    o->iteration_limit = 1000000;
+    o->check_frequency = 64;
+    o->enable_scaling = 1;
+    o->pock_chambolle = 1;
+    o->ruiz_iterations = 10;
+    o->reflection = 1.0;
+    o->mixed_switch_tolerance = 1e-5;
+    o->device = 0;
+    o->autotune = 1;
+    o->verbose = 0;
+}
+
+vajra_status vajra_probe_device(int32_t device, vajra_device_info* info) {
+    if (!info) return VAJRA_ERR_INVALID_ARGUMENT;
+    std::memset(info, 0, sizeof(*info));
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= 0 || device < 0 || device >= count) {
+        cudaGetLastError();
+        std::snprintf(info->device_name, sizeof(info->device_name), "None (No CUDA devices found)");
+        return VAJRA_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        std::snprintf(info->device_name, sizeof(info->device_name), "Error querying CUDA device");
+        return VAJRA_ERR_CUDA;
+    }
+    info->available = 1;
+    std::snprintf(info->device_name, sizeof(info->device_name), "%s", prop.name);
+    info->compute_capability_major = prop.major;
+    info->compute_capability_minor = prop.minor;
+    info->multi_processor_count = prop.multiProcessorCount;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+        info->free_vram_bytes = fr;
+        info->total_vram_bytes = tot;
+    } else {
+        info->total_vram_bytes = prop.totalGlobalMem;
+    }
+    cudaSetDevice(prev);
+    return VAJRA_OK;
+}
+
+int32_t vajra_is_cuda_available(void) {
+    vajra_device_info info;
+    return vajra_probe_device(0, &info) == VAJRA_OK ? 1 : 0;
+}
+
+void vajra_last_timing(vajra_timing* out) {
+    if (out) *out = g_last_timing;
+}
+
+vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra_pdhg** handle) {
+    if (!handle) return VAJRA_ERR_INVALID_ARGUMENT;
+    *handle = nullptr;
+    vajra_status s = validate_host(lp);
+    if (s != VAJRA_OK) return s;
+    vajra_opts o;
+    if (opts) o = *opts; else vajra_default_opts(&o);
+    if (o.algorithm != VAJRA_ALGO_REFERENCE && o.algorithm != VAJRA_ALGO_HALPERN) {
+        set_error("unknown algorithm %d", o.algorithm);
+        return VAJRA_ERR_INVALID_ARGUMENT;
+    }
+    vajra_device_info info;
+    s = vajra_probe_device(o.device, &info);
+    if (s != VAJRA_OK) { set_error("no usable CUDA device %d (no CPU fallback)", o.device); return VAJRA_ERR_NO_DEVICE; }
+    auto t0 = Clock::now();
+    vajra_pdhg* h = new (std::nothrow) vajra_pdhg();
+    if (!h) return VAJRA_ERR_INTERNAL;
+    h->opts = o;
+    h->device = o.device;
+    h->m = lp->num_rows;
+    h->n = lp->num_cols;
+    h->nnz = lp->nnz;
+    h->sense = lp->sense;
+    h->objective_offset = lp->objective_offset;
+    auto fail = [&](vajra_status st) { vajra_pdhg_destroy(h); return st; };
+    if (cudaSetDevice(o.device) != cudaSuccess) return fail(cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__));
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__));
+    if (h->m == 0 || h->n == 0 || (h->nnz == 0 && o.algorithm == VAJRA_ALGO_HALPERN)) {
+        h->h_c.assign(lp->c, lp->c + h->n);
+        h->h_cl.assign(lp->col_lower, lp->col_lower + h->n);
+        h->h_cu.assign(lp->col_upper, lp->col_upper + h->n);
+        h->h_rl.assign(lp->row_lower, lp->row_lower + h->m);
+        h->h_ru.assign(lp->row_upper, lp->row_upper + h->m);
+    }
+    if (h->m > 0 && h->n > 0) {
+        s = upload_lp(lp, h->lp, h->stream);
+        if (s != VAJRA_OK) return fail(s);
+        e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return fail(cuda_status(e, "upload", __FILE__, __LINE__));
+        h->transfers = 8;
+        s = validate_device(h);
+        if (s != VAJRA_OK) return fail(s);
+    }
+    h->upload_time_sec = seconds_since(t0);
+    *handle = h;
+    return VAJRA_OK;
+}
+
+vajra_status vajra_pdhg_destroy(vajra_pdhg* h) {
+    if (!h) return VAJRA_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    {
+        vajra::DeviceLp empty;
+        std::swap(h->lp, empty);   // frees device memory before the stream goes
+    }
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return VAJRA_OK;
+}
+
+// Closed form for nnz == 0 (HALPERN): rows decouple; a row is feasible iff 0 in [l, u].
+static vajra_status solve_no_nonzeros(vajra_pdhg* h, vajra_result* r) {
+    const int m = h->m, n = h->n;
+    for (int i = 0; i < m; ++i) {
+        if (h->h_rl[i] > 1e-7 || h->h_ru[i] < -1e-7) {
+            r->status = 2;   // INFEASIBLE
+            std::snprintf(r->status_message, sizeof(r->status_message), "row %d: 0 outside its bounds", i);
+            return VAJRA_OK;
+        }
+    }
+    vajra_pdhg tmp;
+    tmp.m = 0; tmp.n = n; tmp.sense = h->sense; tmp.objective_offset = h->objective_offset;
+    tmp.h_c = h->h_c; tmp.h_cl = h->h_cl; tmp.h_cu = h->h_cu;
+    double* rv = r->row_value; double* rd = r->row_dual;
+    r->row_value = nullptr; r->row_dual = nullptr;
+    solve_trivial(&tmp, r);
+    r->row_value = rv; r->row_dual = rd;
+    if (rv) for (int i = 0; i < m; ++i) rv[i] = 0.0;
+    if (rd) for (int i = 0; i < m; ++i) rd[i] = 0.0;
+    return VAJRA_OK;
+}
+
+vajra_status vajra_pdhg_run(vajra_pdhg* h, vajra_result* r) {
+    if (!h || !r) return VAJRA_ERR_INVALID_ARGUMENT;
+    const auto t0 = Clock::now();
+    r->status = VAJRA_SOLVE_NOT_SOLVED;
+    r->status_message[0] = '\0';
+    vajra_status s = VAJRA_OK;
+    if (cudaSetDevice(h->device) != cudaSuccess) {
+        s = cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__);
+    } else if (solve_trivial(h, r)) {
+        s = VAJRA_OK;
+    } else if (h->nnz == 0 && h->opts.algorithm == VAJRA_ALGO_HALPERN) {
+        s = solve_no_nonzeros(h, r);
+    } else if (h->opts.algorithm == VAJRA_ALGO_REFERENCE) {
+        s = run_reference(h, r);
+    } else {
+        s = run_halpern(h, r);
+    }
+    if (s != VAJRA_OK) {
+        fail_result(r, s);
+        cudaGetLastError();
+        if (h->stream) cudaStreamSynchronize(h->stream);
+    }
+    r->upload_time_sec = h->upload_time_sec;
+    r->total_time_sec = seconds_since(t0) + h->upload_time_sec;
+    r->host_device_transfers = h->transfers;
+    g_last_timing.upload_time_sec = r->upload_time_sec;
+    g_last_timing.iteration_time_sec = r->iteration_time_sec;
+    g_last_timing.download_time_sec = r->download_time_sec;
+    g_last_timing.total_time_sec = r->total_time_sec;
+    g_last_timing.host_device_transfers = r->host_device_transfers;
+    g_last_timing.iterations = r->iterations;
+    vajra_device_info info;
+    vajra_probe_device(h->device, &info);
+    std::snprintf(g_last_timing.device_name, sizeof(g_last_timing.device_name), "%s", info.device_name);
+    std::snprintf(g_last_timing.kernel_mode, sizeof(g_last_timing.kernel_mode), "%s",
+                  h->opts.algorithm == VAJRA_ALGO_REFERENCE ? "sm100_exact_fp64"
+                  : h->opts.precision == VAJRA_PREC_MIXED ? "sm100_halpern_mixed" : "sm100_halpern_fp64");
+    return s;
+}
+
+vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_result* r) {
+    if (!r) return VAJRA_ERR_INVALID_ARGUMENT;
+    const auto t0 = Clock::now();
+    vajra_pdhg* h = nullptr;
+    vajra_status s = vajra_pdhg_create(lp, opts, &h);
+    if (s != VAJRA_OK) {
+        fail_result(r, s);
+        return s;
+    }
+    s = vajra_pdhg_run(h, r);
+    vajra_pdhg_destroy(h);
+    r->total_time_sec = seconds_since(t0);
+    g_last_timing.total_time_sec = r->total_time_sec;
+    return s;
+}
+
+// ---------------------------------------------------------------------------------------
+// kernel-level entry points
+// ---------------------------------------------------------------------------------------
+}  // extern "C"
+
+namespace vajra {
+namespace {
+
+template <typename T>
+struct EpiPlain {
+    T* out;
+    __device__ bool active() const { return true; }
+    __device__ void operator()(int i, T s) const { out[i] = s; }
+};
+
+__global__ void k_dual_prox(int m, double sigma, const double* __restrict__ w, const double* __restrict__ rl,
+                            const double* __restrict__ ru, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) y[i] = dual_prox_exact(y[i], w[i], sigma, rl[i], ru[i]);
+}
+
+__global__ void k_primal_prox(int n, double tau, const double* __restrict__ v, const double* __restrict__ c,
+                              const double* __restrict__ cl, const double* __restrict__ cu, double* __restrict__ x,
+                              double* __restrict__ xb) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double x_old = x[j];
+    const double x_new = primal_prox_exact(x_old, v[j], c[j], tau, cl[j], cu[j]);
+    x[j] = x_new;
+    xb[j] = extrapolate_exact(x_new, x_old);
+}
+
+struct EpiStepDual {
+    const double* rl; const double* ru; double* y; double* w; double sigma;
+    __device__ bool active() const { return true; }
+    __device__ void operator()(int i, double s) const {
+        w[i] = s;
+        y[i] = dual_prox_exact(y[i], s, sigma, rl[i], ru[i]);
+    }
+};
+
+struct EpiStepPrimal {
+    const double* c; const double* cl; const double* cu; double* x; double* xb; double* v; double tau;
+    __device__ bool active() const { return true; }
+    __device__ void operator()(int j, double s) const {
+        v[j] = s;
+        const double x_old = x[j];
+        const double x_new = primal_prox_exact(x_old, s, c[j], tau, cl[j], cu[j]);
+        x[j] = x_new;
+        xb[j] = extrapolate_exact(x_new, x_old);
+    }
+};
+
+// compute_diagnostics_device_kernel semantics (spmv_kernels.cuh:210-278) with a
+// deterministic single-CTA reduction.
+__global__ void __launch_bounds__(1024)
+k_device_diagnostics(int m, int n, const double* __restrict__ ax, const double* __restrict__ rl,
+                     const double* __restrict__ ru, const double* __restrict__ aty, const double* __restrict__ c,
+                     const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ cl,
+                     const double* __restrict__ cu, vajra_device_diagnostics* out) {
+    __shared__ double red_max[3 * 32];
+    __shared__ double red_sum[32];
+    double mx[3] = {0.0, 0.0, 0.0};   // primal, dual, nan flag
+    double sm[1] = {0.0};
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const double a = ax[i], yi = y[i];
+        if (isnan(a) || isinf(a) || isnan(yi) || isinf(yi)) mx[2] = 1.0;
+        double viol = 0.0;
+        if (a < rl[i]) viol = rl[i] - a;
+        if (a > ru[i]) viol = a - ru[i];
+        if (viol > mx[0]) mx[0] = viol;
+    }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double xj = x[j], cj = c[j], atyj = aty[j];
+        if (isnan(xj) || isinf(xj) || isnan(cj) || isinf(cj) || isnan(atyj) || isinf(atyj)) mx[2] = 1.0;
+        const double lj = cl[j], uj = cu[j];
+        double p = 0.0;
+        if (xj < lj) p = lj - xj;
+        if (xj > uj) p = xj - uj;
+        if (p > mx[0]) mx[0] = p;
+        const double dj = cj + atyj;
+        double d = 0.0;
+        if (xj > lj + 1e-5 && dj > 1e-6) d = dj;
+        if (xj < uj - 1e-5 && dj < -1e-6) d = -dj;
+        if (lj <= -1e20 && uj >= 1e20) d = fabs(dj);
+        if (d > mx[1]) mx[1] = d;
+        sm[0] += cj * xj;
+    }
+    block_reduce<OpMax, double, 3>(mx, red_max);
+    block_reduce<OpSum, double, 1>(sm, red_sum);
+    if (threadIdx.x == 0) {
+        out->primal_residual = mx[0];
+        out->dual_residual = mx[1];
+        out->objective = sm[0];
+        out->duality_gap = 0.0;
+        out->converged = 0;
+        out->numerical_error = mx[2] > 0.0 ? 1 : 0;
+    }
+}
+
+CsrView exact_view(int rows, const int64_t* ptr, const int32_t* idx) {
+    CsrView v;
+    v.rows = rows;
+    v.ptr = ptr;
+    v.idx = idx;
+    v.group = 1;
+    return v;
+}
+
+}  // namespace
+}  // namespace vajra
+
+extern "C" {
+
+#define VJ_STREAM(s) static_cast<cudaStream_t>(s)
+
+vajra_status vajra_csr_spmv_f64(int32_t rows, const int64_t* row_ptr, const int32_t* col_idx, const double* values,
+                                const double* x, double* y, void* stream) {
+    if (rows < 0 || (rows > 0 && (!row_ptr || !col_idx || !values || !x || !y))) return VAJRA_ERR_INVALID_ARGUMENT;
+    launch_spmv_exact<double, false>(exact_view(rows, row_ptr, col_idx), values, x, EpiPlain<double>{y}, VJ_STREAM(stream));
+    VJ_LAUNCH_CHECK();
+    return VAJRA_OK;
+}
+
+vajra_status vajra_csr_spmv_f32(int32_t rows, const int64_t* row_ptr, const int32_t* col_idx, const float* values,
+                                const float* x, float* y, void* stream) {
+    if (rows < 0 || (rows > 0 && (!row_ptr || !col_idx || !values || !x || !y))) return VAJRA_ERR_INVALID_ARGUMENT;
+    launch_spmv_exact<float, false>(exact_view(rows, row_ptr, col_idx), values, x, EpiPlain<float>{y}, VJ_STREAM(stream));
+    VJ_LAUNCH_CHECK();
+    return VAJRA_OK;
+}
+
+vajra_status vajra_csc_spmv_transpose_f64(int32_t cols, const int64_t* col_ptr, const int32_t* row_idx,
+                                          const double* values, const double* y, double* v, void* stream) {
+    return vajra_csr_spmv_f64(cols, col_ptr, row_idx, values, y, v, stream);
+}
+
+vajra_status vajra_csc_spmv_transpose_f32(int32_t cols, const int64_t* col_ptr, const int32_t* row_idx,
+                                          const float* values, const float* y, float* v, void* stream) {
+    return vajra_csr_spmv_f32(cols, col_ptr, row_idx, values, y, v, stream);
+}
+
+vajra_status vajra_dual_prox_f64(int32_t rows, double sigma, const double* ax, const double* row_lower,
+                                 const double* row_upper, double* y, void* stream) {
+    if (rows < 0 || (rows > 0 && (!ax || !row_lower || !row_upper || !y))) return VAJRA_ERR_INVALID_ARGUMENT;
+    if (rows > 0) k_dual_prox<<<grid_for(rows), kThreads, 0, VJ_STREAM(stream)>>>(rows, sigma, ax, row_lower, row_upper, y);
+    VJ_LAUNCH_CHECK();
+    return VAJRA_OK;
+}
+
+vajra_status vajra_primal_prox_f64(int32_t cols, double tau, const double* aty, const double* c,
+                                   const double* col_lower, const double* col_upper, double* x, double* x_bar,
+                                   void* stream) {
+    if (cols < 0 || (cols > 0 && (!aty || !c || !col_lower || !col_upper || !x || !x_bar))) return VAJRA_ERR_INVALID_ARGUMENT;
+    if (cols > 0) k_primal_prox<<<grid_for(cols), kThreads, 0, VJ_STREAM(stream)>>>(cols, tau, aty, c, col_lower, col_upper, x, x_bar);
+    VJ_LAUNCH_CHECK();
+    return VAJRA_OK;
+}
+
+vajra_status vajra_device_diagnostics_f64(int32_t rows, int32_t cols, const double* ax, const double* row_lower,
+                                          const double* row_upper, const double* aty, const double* c,
+                                          const double* x, const double* y, const double* col_lower,
+                                          const double* col_upper, vajra_device_diagnostics* out, void* stream) {
+    if (rows < 0 || cols < 0 || !out) return VAJRA_ERR_INVALID_ARGUMENT;
+    k_device_diagnostics<<<1, 1024, 0, VJ_STREAM(stream)>>>(rows, cols, ax, row_lower, row_upper, aty, c, x, y,
+                                                           col_lower, col_upper, out);
+    VJ_LAUNCH_CHECK();
+    return VAJRA_OK;
+}
+
+vajra_status vajra_pdhg_step_f64(int32_t rows, int32_t cols, const int64_t* row_ptr, const int32_t* col_idx,
+                                 const double* csr_values, const int64_t* col_ptr, const int32_t* row_idx,
+                                 const double* csc_values, const double* row_lower, const double* row_upper,
+                                 const double* c, const double* col_lower, const double* col_upper, double sigma,
+                                 double tau, double* x, double* x_bar, double* y, double* w, double* v,
+                                 void* stream) {
+    if (rows < 0 || cols < 0) return VAJRA_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = VJ_STREAM(stream);
+    launch_spmv_exact<double, false>(exact_view(rows, row_ptr, col_idx), csr_values, x_bar,
+                                     EpiStepDual{row_lower, row_upper, y, w, sigma}, st);
+    launch_spmv_exact<double, false>(exact_view(cols, col_ptr, row_idx), csc_values, y,
+                                     EpiStepPrimal{c, col_lower, col_upper, x, x_bar, v, tau}, st);
+    VJ_LAUNCH_CHECK();
+    return VAJRA_OK;
+}
+
+}  // extern "C"

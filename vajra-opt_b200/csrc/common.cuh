@@ -1,0 +1,128 @@
+// Shared infrastructure for libvajra_pdhg: status plumbing (no exception ever crosses the C
+// ABI), owning device buffers, and deterministic reductions (fixed order, no atomics on
+// floating-point values, so every run repeats bit for bit).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "vajra_pdhg.h"
+
+namespace vajra {
+
+// Last error text of the calling thread (copied into vajra_result::status_message).
+void set_error(const char* fmt, ...);
+const char* last_error();
+
+vajra_status cuda_status(cudaError_t e, const char* what, const char* file, int line);
+
+#define VJ_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t vj_e_ = (call);                                                    \
+        if (vj_e_ != cudaSuccess) return ::vajra::cuda_status(vj_e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define VJ_TRY(call)                                                                   \
+    do {                                                                               \
+        vajra_status vj_s_ = (call);                                                   \
+        if (vj_s_ != VAJRA_OK) return vj_s_;                                           \
+    } while (0)
+
+#define VJ_LAUNCH_CHECK() VJ_CUDA(cudaGetLastError())
+
+constexpr int kThreads = 256;           // default CTA size of elementwise / SpMV kernels
+constexpr double kInf = 1e20;           // reference infinity convention (model.hpp)
+constexpr double kZeroDrop = 1e-11;     // tol::kZeroDrop (tolerances.hpp:28)
+
+inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 << 30) {
+    int64_t g = (work + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return static_cast<unsigned>(g);
+}
+
+// Owning device allocation.  Moves only; frees on destruction.
+template <typename T>
+class DeviceBuffer {
+public:
+    DeviceBuffer() = default;
+    ~DeviceBuffer() { reset(); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) { reset(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+        return *this;
+    }
+    vajra_status alloc(size_t n) {
+        reset();
+        if (n == 0) n = 1;   // keep a valid pointer for empty extents
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p_), n * sizeof(T));
+        if (e != cudaSuccess) { p_ = nullptr; return cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
+        n_ = n;
+        return VAJRA_OK;
+    }
+    void reset() noexcept {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T* get() const noexcept { return p_; }
+    size_t size() const noexcept { return n_; }
+
+private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+// ---------------------------------------------------------------------------------------
+// Deterministic reductions.  A warp reduces with an xor butterfly, a block combines its
+// warps in warp order through shared memory, and a grid combines per-block partials in
+// block order in a second single-CTA pass.  Same inputs -> same bits on every run.
+// ---------------------------------------------------------------------------------------
+struct OpSum {
+    template <typename T> __device__ static T apply(T a, T b) { return a + b; }
+    template <typename T> __device__ static T identity() { return T(0); }
+};
+struct OpMax {   // ignores NaN like `if (v > cur) cur = v`
+    template <typename T> __device__ static T apply(T a, T b) { return (b > a) ? b : a; }
+    template <typename T> __device__ static T identity() { return T(0); }
+};
+
+template <class Op, typename T>
+__device__ __forceinline__ T warp_reduce(T v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = Op::apply(v, __shfl_xor_sync(0xffffffffu, v, off));
+    return v;
+}
+
+// Reduces NV values per thread across the block; the result is valid in thread 0.
+// `smem` must hold NV * 32 values.  All threads of the block must call it.
+template <class Op, typename T, int NV>
+__device__ __forceinline__ void block_reduce(T (&v)[NV], T* smem) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = warp_reduce<Op>(v[q]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) smem[q * 32 + warp] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            T acc = smem[q * 32];
+            for (int w = 1; w < nwarps; ++w) acc = Op::apply(acc, smem[q * 32 + w]);
+            v[q] = acc;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace vajra

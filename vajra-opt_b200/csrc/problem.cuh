@@ -1,0 +1,96 @@
+// Device-resident LP data and the set-up passes that turn the caller's CSC into what the
+// iteration kernels read.
+//
+// HBM layout (one LP, one device):
+//   raw (uploaded once by vajra_pdhg_create, never modified):
+//     col_ptr int64[n+1] | row_idx int32[nnz] | values f64[nnz] | c, col_lo, col_up f64[n]
+//     | row_lo, row_up f64[m]
+//   prepared (rebuilt by every run; the reference does this on the host, pdhg_cuda.cu:136-171):
+//     CSR of A: csr_ptr int64[m+1] | csr_idx int32[nnz] | perm int64[nnz] (CSR slot -> CSC slot)
+//     scaled values in both orders (f64; plus f32 copies for the mixed-precision path)
+//     scaled c (negated for maximisation), bounds, cumulative row / column scales.
+#pragma once
+
+#include "common.cuh"
+#include "spmv.cuh"
+
+namespace vajra {
+
+struct DeviceLp {
+    int m = 0, n = 0;
+    int64_t nnz = 0;
+    int sense = 0;
+    double objective_offset = 0.0;
+    DeviceBuffer<int64_t> col_ptr;
+    DeviceBuffer<int32_t> row_idx;
+    DeviceBuffer<double> values;
+    DeviceBuffer<double> c, col_lower, col_upper, row_lower, row_upper;
+};
+
+struct Prepared {
+    // structure
+    DeviceBuffer<int64_t> csr_ptr;
+    DeviceBuffer<int32_t> csr_idx;
+    DeviceBuffer<int64_t> perm;
+    // scaled data (CSC order = stored transpose, CSR order = A)
+    DeviceBuffer<double> csc_val, csr_val;
+    DeviceBuffer<float> csc_val32, csr_val32;
+    DeviceBuffer<double> csr_val_orig;       // unscaled A in CSR order (post-processing)
+    DeviceBuffer<double> c, col_lower, col_upper, row_lower, row_upper;
+    DeviceBuffer<double> row_scale, col_scale;
+    // per-row / per-column lists of long rows for the fast SpMV
+    DeviceBuffer<int32_t> long_rows_a, long_rows_at;
+    bool scaled = false;
+    CsrView a, at;                            // A (rows = m) and A^T (rows = n)
+};
+
+// Scalars that set-up passes hand to one another on the device.
+struct SetupState {
+    int ruiz_done;
+    int power_done;
+    double ruiz_row_err;
+    double ruiz_col_err;
+    double lambda;
+    double lambda_prev;
+    double inv_norm;
+    double spectral_norm;
+    int power_iter;
+    int pad;
+};
+
+vajra_status upload_lp(const vajra_lp* lp, DeviceLp& d, cudaStream_t st);
+
+// CSC -> CSR structure (stable radix sort by row keeps columns ascending within a row).
+vajra_status build_csr(const DeviceLp& lp, Prepared& p, cudaStream_t st);
+
+struct ScalingOpts {
+    bool enable = true;
+    int ruiz_iterations = 10;
+    double ruiz_tolerance = 0.05;
+    bool pock_chambolle = false;
+    bool negate_c = false;     // maximisation
+};
+
+// Copies the raw data into the working buffers and applies Ruiz (exactly as
+// src/linalg/scaling.cpp:7-153) and optionally Pock-Chambolle (alpha = 1) scaling, then
+// fills the CSR-ordered values.  `sst` is a device SetupState.
+vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& o,
+                            SetupState* sst, cudaStream_t st);
+
+// f32 copies of the scaled values (mixed-precision path).
+vajra_status make_f32_values(Prepared& p, int64_t nnz, cudaStream_t st);
+
+// Reference power iteration (src/solvers/pdhg/pdhg.cpp:11-56) evaluated in its order:
+// sequential sums, zero-drop skip.  Result in sst->spectral_norm.
+vajra_status spectral_norm_exact(const Prepared& p, int m, int n, int max_iter, double tol,
+                                 SetupState* sst, cudaStream_t st);
+
+// Fast power iteration on the scaled A (fp64, deterministic tree sums).
+vajra_status spectral_norm_fast(const Prepared& p, int m, int n, int max_iter, double tol,
+                                SetupState* sst, cudaStream_t st);
+
+// Long-row lists and group sizes for the fast SpMV (a heuristic; the solver's autotuner
+// may override `group`).
+vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st);
+
+}  // namespace vajra

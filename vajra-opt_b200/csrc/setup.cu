@@ -1,0 +1,482 @@
+// Device set-up passes: upload, CSC -> CSR, Ruiz / Pock-Chambolle scaling, power iteration.
+// The reference runs all of this single-threaded on the host before the first iteration
+// (src/solvers/gpu/pdhg_cuda.cu:136-171); here it stays on the device.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <cmath>
+
+#include "problem.cuh"
+
+namespace vajra {
+
+// ---------------------------------------------------------------------------------------
+// upload
+// ---------------------------------------------------------------------------------------
+template <typename T>
+static vajra_status upload(DeviceBuffer<T>& d, const T* h, size_t n, cudaStream_t st) {
+    VJ_TRY(d.alloc(n));
+    if (n) VJ_CUDA(cudaMemcpyAsync(d.get(), h, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    return VAJRA_OK;
+}
+
+vajra_status upload_lp(const vajra_lp* lp, DeviceLp& d, cudaStream_t st) {
+    d.m = lp->num_rows;
+    d.n = lp->num_cols;
+    d.nnz = lp->col_ptr[lp->num_cols];
+    d.sense = lp->sense;
+    d.objective_offset = lp->objective_offset;
+    VJ_TRY(upload(d.col_ptr, lp->col_ptr, static_cast<size_t>(d.n) + 1, st));
+    VJ_TRY(upload(d.row_idx, lp->row_idx, static_cast<size_t>(d.nnz), st));
+    VJ_TRY(upload(d.values, lp->values, static_cast<size_t>(d.nnz), st));
+    VJ_TRY(upload(d.c, lp->c, static_cast<size_t>(d.n), st));
+    VJ_TRY(upload(d.col_lower, lp->col_lower, static_cast<size_t>(d.n), st));
+    VJ_TRY(upload(d.col_upper, lp->col_upper, static_cast<size_t>(d.n), st));
+    VJ_TRY(upload(d.row_lower, lp->row_lower, static_cast<size_t>(d.m), st));
+    VJ_TRY(upload(d.row_upper, lp->row_upper, static_cast<size_t>(d.m), st));
+    return VAJRA_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// CSC -> CSR
+// ---------------------------------------------------------------------------------------
+__global__ void k_expand_cols(int n, const int64_t* __restrict__ col_ptr, int32_t* __restrict__ col_of) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) col_of[k] = j;
+}
+
+__global__ void k_iota64(int64_t nnz, int64_t* __restrict__ v) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nnz;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        v[k] = k;
+}
+
+// row_ptr[r] = first k with keys[k] >= r (keys sorted ascending); each r written once.
+__global__ void k_row_ptr_from_sorted(int64_t nnz, int m, const int32_t* __restrict__ keys,
+                                      int64_t* __restrict__ row_ptr) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k <= nnz;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int lo = (k == 0) ? -1 : keys[k - 1];
+        const int hi = (k == nnz) ? m : keys[k];
+        for (int r = lo + 1; r <= hi; ++r) row_ptr[r] = k;
+    }
+}
+
+template <typename T>
+__global__ void k_gather(int64_t nnz, const int64_t* __restrict__ perm, const T* __restrict__ src,
+                         T* __restrict__ dst) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nnz;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[k] = src[perm[k]];
+}
+
+template <typename Ti, typename To>
+__global__ void k_convert(int64_t n, const Ti* __restrict__ src, To* __restrict__ dst) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[k] = static_cast<To>(src[k]);
+}
+
+static unsigned grid_stride_blocks(int64_t work) { return grid_for(work, kThreads, 148 * 32); }
+
+vajra_status build_csr(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
+    const int m = lp.m, n = lp.n;
+    const int64_t nnz = lp.nnz;
+    VJ_TRY(p.csr_ptr.alloc(static_cast<size_t>(m) + 1));
+    VJ_TRY(p.csr_idx.alloc(static_cast<size_t>(nnz)));
+    VJ_TRY(p.perm.alloc(static_cast<size_t>(nnz)));
+    DeviceBuffer<int32_t> col_of, keys_out;
+    DeviceBuffer<int64_t> iota;
+    VJ_TRY(col_of.alloc(static_cast<size_t>(nnz)));
+    VJ_TRY(keys_out.alloc(static_cast<size_t>(nnz)));
+    VJ_TRY(iota.alloc(static_cast<size_t>(nnz)));
+    if (n > 0) k_expand_cols<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), col_of.get());
+    k_iota64<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, iota.get());
+    VJ_LAUNCH_CHECK();
+    if (nnz > 0) {
+        int end_bit = 1;
+        while (end_bit < 31 && (1LL << end_bit) < m) ++end_bit;
+        size_t temp_bytes = 0;
+        VJ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, lp.row_idx.get(), keys_out.get(),
+                                                iota.get(), p.perm.get(), nnz, 0, end_bit, st));
+        DeviceBuffer<unsigned char> temp;
+        VJ_TRY(temp.alloc(temp_bytes));
+        VJ_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), temp_bytes, lp.row_idx.get(), keys_out.get(),
+                                                iota.get(), p.perm.get(), nnz, 0, end_bit, st));
+        k_gather<int32_t><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.perm.get(), col_of.get(), p.csr_idx.get());
+    }
+    k_row_ptr_from_sorted<<<grid_stride_blocks(nnz + 1), kThreads, 0, st>>>(nnz, m, keys_out.get(), p.csr_ptr.get());
+    VJ_LAUNCH_CHECK();
+    // Keep the temporaries alive until the work that reads them has run.
+    VJ_CUDA(cudaStreamSynchronize(st));
+    return VAJRA_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// scaling (Ruiz: src/linalg/scaling.cpp:7-153, in its evaluation order)
+// ---------------------------------------------------------------------------------------
+__global__ void k_col_inf(int n, const int64_t* __restrict__ col_ptr, const double* __restrict__ v,
+                          double* __restrict__ col_inf, const SetupState* sst) {
+    if (sst->ruiz_done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double mx = 0.0;
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+        const double a = fabs(v[k]);
+        if (a > mx) mx = a;
+    }
+    col_inf[j] = mx;
+}
+
+__global__ void k_row_inf(int m, const int64_t* __restrict__ csr_ptr, const int64_t* __restrict__ perm,
+                          const double* __restrict__ v, double* __restrict__ row_inf, const SetupState* sst) {
+    if (sst->ruiz_done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    double mx = 0.0;
+    for (int64_t k = csr_ptr[i]; k < csr_ptr[i + 1]; ++k) {
+        const double a = fabs(v[perm[k]]);
+        if (a > mx) mx = a;
+    }
+    row_inf[i] = mx;
+}
+
+// One CTA: max |1 - inf| over rows / columns with inf > 1e-11, then the convergence test.
+__global__ void k_ruiz_err(int m, int n, const double* __restrict__ row_inf, const double* __restrict__ col_inf,
+                           double tol, SetupState* sst) {
+    if (sst->ruiz_done) return;
+    __shared__ double red[2 * 32];
+    double v[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        if (row_inf[i] > kZeroDrop) { const double e = fabs(1.0 - row_inf[i]); if (e > v[0]) v[0] = e; }
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+        if (col_inf[j] > kZeroDrop) { const double e = fabs(1.0 - col_inf[j]); if (e > v[1]) v[1] = e; }
+    block_reduce<OpMax, double, 2>(v, red);
+    if (threadIdx.x == 0) {
+        sst->ruiz_row_err = v[0];
+        sst->ruiz_col_err = v[1];
+        if (v[0] <= tol && v[1] <= tol) sst->ruiz_done = 1;
+    }
+}
+
+// r = 1/sqrt(norm) (1 where norm <= 1e-11); cumulative scale *= r.
+__global__ void k_scale_factors(int k_count, const double* __restrict__ norm, double* __restrict__ step,
+                                double* __restrict__ scale, const SetupState* sst, int respect_done) {
+    if (respect_done && sst->ruiz_done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k_count) return;
+    const double r = (norm[i] > kZeroDrop) ? __ddiv_rn(1.0, __dsqrt_rn(norm[i])) : 1.0;
+    step[i] = r;
+    scale[i] = __dmul_rn(scale[i], r);
+}
+
+// A_ij *= r_i * c_j (scaling.cpp:92-100: the product of the two factors first).
+__global__ void k_scale_matrix(int n, const int64_t* __restrict__ col_ptr, const int32_t* __restrict__ row_idx,
+                               double* __restrict__ v, const double* __restrict__ r, const double* __restrict__ cs,
+                               const SetupState* sst, int respect_done) {
+    if (respect_done && sst->ruiz_done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double cj = cs[j];
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) v[k] = __dmul_rn(v[k], __dmul_rn(r[row_idx[k]], cj));
+}
+
+// Pock-Chambolle (alpha = 1) norms: sum |a| per column / per row, in storage order.
+__global__ void k_col_abs_sum(int n, const int64_t* __restrict__ col_ptr, const double* __restrict__ v,
+                              double* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double s = 0.0;
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) s += fabs(v[k]);
+    out[j] = s;
+}
+
+__global__ void k_row_abs_sum(int m, const int64_t* __restrict__ csr_ptr, const int64_t* __restrict__ perm,
+                              const double* __restrict__ v, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    double s = 0.0;
+    for (int64_t k = csr_ptr[i]; k < csr_ptr[i + 1]; ++k) s += fabs(v[perm[k]]);
+    out[i] = s;
+}
+
+// c *= C; finite row bounds *= R; finite column bounds *= C^-1 (scaling.cpp:104-149).
+__global__ void k_scale_vectors(int m, int n, double* c, double* rl, double* ru, double* cl, double* cu,
+                                const double* __restrict__ rs, const double* __restrict__ cs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        c[i] = __dmul_rn(c[i], cs[i]);
+        const double inv = __ddiv_rn(1.0, cs[i]);
+        if (cl[i] > -kInf) cl[i] = __dmul_rn(cl[i], inv);
+        if (cu[i] < kInf) cu[i] = __dmul_rn(cu[i], inv);
+    }
+    if (i < m) {
+        if (rl[i] > -kInf) rl[i] = __dmul_rn(rl[i], rs[i]);
+        if (ru[i] < kInf) ru[i] = __dmul_rn(ru[i], rs[i]);
+    }
+}
+
+__global__ void k_fill(int64_t n, double* v, double val) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        v[k] = val;
+}
+
+__global__ void k_negate(int n, double* v) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) v[j] = -v[j];
+}
+
+vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& o, SetupState* sst,
+                            cudaStream_t st) {
+    const int m = lp.m, n = lp.n;
+    const int64_t nnz = lp.nnz;
+    auto copy = [&](DeviceBuffer<double>& dst, const DeviceBuffer<double>& src, size_t cnt) -> vajra_status {
+        VJ_TRY(dst.alloc(cnt));
+        if (cnt) VJ_CUDA(cudaMemcpyAsync(dst.get(), src.get(), cnt * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        return VAJRA_OK;
+    };
+    VJ_TRY(copy(p.csc_val, lp.values, static_cast<size_t>(nnz)));
+    VJ_TRY(copy(p.c, lp.c, static_cast<size_t>(n)));
+    VJ_TRY(copy(p.col_lower, lp.col_lower, static_cast<size_t>(n)));
+    VJ_TRY(copy(p.col_upper, lp.col_upper, static_cast<size_t>(n)));
+    VJ_TRY(copy(p.row_lower, lp.row_lower, static_cast<size_t>(m)));
+    VJ_TRY(copy(p.row_upper, lp.row_upper, static_cast<size_t>(m)));
+    VJ_TRY(p.row_scale.alloc(static_cast<size_t>(m)));
+    VJ_TRY(p.col_scale.alloc(static_cast<size_t>(n)));
+    k_fill<<<grid_stride_blocks(m), kThreads, 0, st>>>(m, p.row_scale.get(), 1.0);
+    k_fill<<<grid_stride_blocks(n), kThreads, 0, st>>>(n, p.col_scale.get(), 1.0);
+    if (o.negate_c && n > 0) k_negate<<<grid_for(n), kThreads, 0, st>>>(n, p.c.get());
+    VJ_LAUNCH_CHECK();
+    p.scaled = false;
+    if (o.enable && m > 0 && n > 0) {
+        DeviceBuffer<double> row_norm, col_norm, r_k, c_k;
+        VJ_TRY(row_norm.alloc(static_cast<size_t>(m)));
+        VJ_TRY(col_norm.alloc(static_cast<size_t>(n)));
+        VJ_TRY(r_k.alloc(static_cast<size_t>(m)));
+        VJ_TRY(c_k.alloc(static_cast<size_t>(n)));
+        VJ_CUDA(cudaMemsetAsync(sst, 0, sizeof(SetupState), st));
+        for (int it = 0; it < o.ruiz_iterations; ++it) {
+            k_col_inf<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), p.csc_val.get(), col_norm.get(), sst);
+            k_row_inf<<<grid_for(m), kThreads, 0, st>>>(m, p.csr_ptr.get(), p.perm.get(), p.csc_val.get(),
+                                                        row_norm.get(), sst);
+            k_ruiz_err<<<1, 1024, 0, st>>>(m, n, row_norm.get(), col_norm.get(), o.ruiz_tolerance, sst);
+            k_scale_factors<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(), sst, 1);
+            k_scale_factors<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(), sst, 1);
+            k_scale_matrix<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), lp.row_idx.get(), p.csc_val.get(),
+                                                             r_k.get(), c_k.get(), sst, 1);
+            VJ_LAUNCH_CHECK();
+        }
+        if (o.pock_chambolle) {
+            k_col_abs_sum<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), p.csc_val.get(), col_norm.get());
+            k_row_abs_sum<<<grid_for(m), kThreads, 0, st>>>(m, p.csr_ptr.get(), p.perm.get(), p.csc_val.get(), row_norm.get());
+            k_scale_factors<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(), sst, 0);
+            k_scale_factors<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(), sst, 0);
+            k_scale_matrix<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), lp.row_idx.get(), p.csc_val.get(),
+                                                             r_k.get(), c_k.get(), sst, 0);
+            VJ_LAUNCH_CHECK();
+        }
+        const int mx = m > n ? m : n;
+        k_scale_vectors<<<grid_for(mx), kThreads, 0, st>>>(m, n, p.c.get(), p.row_lower.get(), p.row_upper.get(),
+                                                           p.col_lower.get(), p.col_upper.get(),
+                                                           p.row_scale.get(), p.col_scale.get());
+        VJ_LAUNCH_CHECK();
+        VJ_CUDA(cudaStreamSynchronize(st));   // temporaries above go out of scope
+        p.scaled = true;
+    }
+    VJ_TRY(p.csr_val.alloc(static_cast<size_t>(nnz)));
+    VJ_TRY(p.csr_val_orig.alloc(static_cast<size_t>(nnz)));
+    if (nnz > 0) {
+        k_gather<double><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.perm.get(), p.csc_val.get(), p.csr_val.get());
+        k_gather<double><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.perm.get(), lp.values.get(), p.csr_val_orig.get());
+        VJ_LAUNCH_CHECK();
+    }
+    // CSR views: A over csr_*, A^T over the raw CSC structure.
+    p.a.rows = m; p.a.cols = n; p.a.nnz = nnz; p.a.ptr = p.csr_ptr.get(); p.a.idx = p.csr_idx.get();
+    p.at.rows = n; p.at.cols = m; p.at.nnz = nnz; p.at.ptr = lp.col_ptr.get(); p.at.idx = lp.row_idx.get();
+    return VAJRA_OK;
+}
+
+vajra_status make_f32_values(Prepared& p, int64_t nnz, cudaStream_t st) {
+    VJ_TRY(p.csc_val32.alloc(static_cast<size_t>(nnz)));
+    VJ_TRY(p.csr_val32.alloc(static_cast<size_t>(nnz)));
+    if (nnz > 0) {
+        k_convert<double, float><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.csc_val.get(), p.csc_val32.get());
+        k_convert<double, float><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.csr_val.get(), p.csr_val32.get());
+        VJ_LAUNCH_CHECK();
+    }
+    return VAJRA_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// power iteration (src/solvers/pdhg/pdhg.cpp:11-56)
+// ---------------------------------------------------------------------------------------
+struct EpiStoreUnlessDone {
+    double* out;
+    const int* done;
+    __device__ bool active() const { return *done == 0; }
+    __device__ void operator()(int row, double s) const { out[row] = s; }
+};
+
+// Sequential: the reference sums u_j^2 in index order.
+__global__ void k_power_step_exact(int n, const double* __restrict__ u, double tol, SetupState* sst) {
+    if (sst->power_done) return;
+    double norm_sq = 0.0;
+    for (int j = 0; j < n; ++j) norm_sq = __dadd_rn(norm_sq, __dmul_rn(u[j], u[j]));
+    const double norm = __dsqrt_rn(norm_sq);
+    const int it = sst->power_iter;
+    if (norm < 1e-15 || isnan(norm) || isinf(norm)) {
+        sst->spectral_norm = (sst->lambda > 1e-6) ? __dsqrt_rn(sst->lambda) : 1e-3;
+        sst->power_done = 2;   // 2: result already final
+        return;
+    }
+    sst->lambda = norm;
+    if (it > 0 && fabs(__dsub_rn(norm, sst->lambda_prev)) <= __dmul_rn(tol, norm)) {
+        sst->power_done = 1;
+        return;
+    }
+    sst->lambda_prev = norm;
+    sst->inv_norm = __ddiv_rn(1.0, norm);
+    sst->power_iter = it + 1;
+}
+
+__global__ void k_power_scale(int n, const double* __restrict__ u, double* __restrict__ v, const SetupState* sst) {
+    if (sst->power_done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) v[j] = __dmul_rn(u[j], sst->inv_norm);
+}
+
+__global__ void k_power_final(SetupState* sst) {
+    if (sst->power_done == 2) return;
+    const double s = __dsqrt_rn(sst->lambda);
+    sst->spectral_norm = (s > 1e-12) ? s : 1e-6;
+}
+
+static vajra_status power_init(int n, DeviceBuffer<double>& v, DeviceBuffer<double>& w, DeviceBuffer<double>& u,
+                               int m, SetupState* sst, cudaStream_t st) {
+    VJ_TRY(v.alloc(static_cast<size_t>(n)));
+    VJ_TRY(w.alloc(static_cast<size_t>(m)));
+    VJ_TRY(u.alloc(static_cast<size_t>(n)));
+    const double v0 = 1.0 / std::sqrt(static_cast<double>(n));
+    k_fill<<<grid_stride_blocks(n), kThreads, 0, st>>>(n, v.get(), v0);
+    SetupState init{};
+    init.lambda = 1.0;
+    VJ_CUDA(cudaMemcpyAsync(sst, &init, sizeof(SetupState), cudaMemcpyHostToDevice, st));
+    VJ_CUDA(cudaStreamSynchronize(st));   // `init` lives on this stack frame
+    return VAJRA_OK;
+}
+
+vajra_status spectral_norm_exact(const Prepared& p, int m, int n, int max_iter, double tol, SetupState* sst,
+                                 cudaStream_t st) {
+    DeviceBuffer<double> v, w, u;
+    VJ_TRY(power_init(n, v, w, u, m, sst, st));
+    const int* done = &sst->power_done;
+    for (int it = 0; it < max_iter; ++it) {
+        launch_spmv_exact<double, true>(p.a, p.csr_val.get(), v.get(), EpiStoreUnlessDone{w.get(), done}, st);
+        launch_spmv_exact<double, false>(p.at, p.csc_val.get(), w.get(), EpiStoreUnlessDone{u.get(), done}, st);
+        k_power_step_exact<<<1, 1, 0, st>>>(n, u.get(), tol, sst);
+        k_power_scale<<<grid_for(n), kThreads, 0, st>>>(n, u.get(), v.get(), sst);
+        VJ_LAUNCH_CHECK();
+    }
+    k_power_final<<<1, 1, 0, st>>>(sst);
+    VJ_LAUNCH_CHECK();
+    VJ_CUDA(cudaStreamSynchronize(st));
+    return VAJRA_OK;
+}
+
+// Fast form: deterministic two-stage sum of squares.
+__global__ void k_sumsq_partial(int n, const double* __restrict__ u, double* __restrict__ part, const SetupState* sst) {
+    if (sst->power_done) return;
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) v[0] += u[j] * u[j];
+    block_reduce<OpSum, double, 1>(v, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+__global__ void k_power_step_fast(int nparts, const double* __restrict__ part, double tol, SetupState* sst) {
+    if (sst->power_done) return;
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) v[0] += part[b];
+    block_reduce<OpSum, double, 1>(v, red);
+    if (threadIdx.x != 0) return;
+    const double norm = sqrt(v[0]);
+    const int it = sst->power_iter;
+    if (norm < 1e-15 || isnan(norm) || isinf(norm)) {
+        sst->spectral_norm = (sst->lambda > 1e-6) ? sqrt(sst->lambda) : 1e-3;
+        sst->power_done = 2;
+        return;
+    }
+    sst->lambda = norm;
+    if (it > 0 && fabs(norm - sst->lambda_prev) <= tol * norm) { sst->power_done = 1; return; }
+    sst->lambda_prev = norm;
+    sst->inv_norm = 1.0 / norm;
+    sst->power_iter = it + 1;
+}
+
+vajra_status spectral_norm_fast(const Prepared& p, int m, int n, int max_iter, double tol, SetupState* sst,
+                                cudaStream_t st) {
+    DeviceBuffer<double> v, w, u, part;
+    VJ_TRY(power_init(n, v, w, u, m, sst, st));
+    const int nparts = 148 * 4;
+    VJ_TRY(part.alloc(nparts));
+    const int* done = &sst->power_done;
+    for (int it = 0; it < max_iter; ++it) {
+        launch_spmv<double, double>(p.a, p.csr_val.get(), v.get(), EpiStoreUnlessDone{w.get(), done}, st);
+        launch_spmv<double, double>(p.at, p.csc_val.get(), w.get(), EpiStoreUnlessDone{u.get(), done}, st);
+        k_sumsq_partial<<<nparts, kThreads, 0, st>>>(n, u.get(), part.get(), sst);
+        k_power_step_fast<<<1, kThreads, 0, st>>>(nparts, part.get(), tol, sst);
+        k_power_scale<<<grid_for(n), kThreads, 0, st>>>(n, u.get(), v.get(), sst);
+        VJ_LAUNCH_CHECK();
+    }
+    k_power_final<<<1, 1, 0, st>>>(sst);
+    VJ_LAUNCH_CHECK();
+    VJ_CUDA(cudaStreamSynchronize(st));
+    return VAJRA_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// SpMV plan: group size from the mean row length, long-row lists
+// ---------------------------------------------------------------------------------------
+__global__ void k_collect_long(int rows, const int64_t* __restrict__ ptr, int64_t long_len,
+                               int32_t* __restrict__ out, int* __restrict__ count) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    if (ptr[r + 1] - ptr[r] > long_len) out[atomicAdd(count, 1)] = r;
+}
+
+static int default_group(double mean_len) {
+    int g = 1;
+    while (g < 32 && g * 2 <= mean_len) g *= 2;   // ~2 products per lane
+    return g;
+}
+
+static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, cudaStream_t st) {
+    const double mean = v.rows > 0 ? static_cast<double>(v.nnz) / v.rows : 0.0;
+    v.group = default_group(mean);
+    int64_t long_len = static_cast<int64_t>(8.0 * mean);
+    if (long_len < 256) long_len = 256;
+    v.long_len = long_len;
+    VJ_TRY(list.alloc(static_cast<size_t>(v.rows > 0 ? v.rows : 1)));
+    DeviceBuffer<int> cnt;
+    VJ_TRY(cnt.alloc(1));
+    VJ_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int), st));
+    if (v.rows > 0) k_collect_long<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, long_len, list.get(), cnt.get());
+    VJ_LAUNCH_CHECK();
+    int h = 0;
+    VJ_CUDA(cudaMemcpyAsync(&h, cnt.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    v.n_long = h;
+    v.long_rows = list.get();
+    return VAJRA_OK;
+}
+
+vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
+    (void)lp;
+    VJ_TRY(plan_one(p.a, p.long_rows_a, st));
+    VJ_TRY(plan_one(p.at, p.long_rows_at, st));
+    return VAJRA_OK;
+}
+
+}  // namespace vajra

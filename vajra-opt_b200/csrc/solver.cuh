@@ -1,0 +1,45 @@
+// The opaque vajra_pdhg handle and the two solver drivers.
+#pragma once
+
+#include <chrono>
+#include <vector>
+
+#include "problem.cuh"
+
+struct vajra_pdhg {
+    vajra_opts opts{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    vajra::DeviceLp lp;
+    // host copies needed for closed-form trivial cases and post-processing sizes
+    int m = 0, n = 0;
+    int64_t nnz = 0;
+    int sense = 0;
+    double objective_offset = 0.0;
+    std::vector<double> h_c, h_cl, h_cu, h_rl, h_ru;   // only kept for m == 0 / nnz == 0
+    double upload_time_sec = 0.0;
+    int64_t transfers = 0;
+};
+
+namespace vajra {
+
+using Clock = std::chrono::steady_clock;
+inline double seconds_since(Clock::time_point t0) {
+    return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+// Copies result vectors / scalars to the caller and records the timing.
+struct HostOut {
+    vajra_result* r;
+};
+
+vajra_status run_reference(vajra_pdhg* h, vajra_result* r);
+vajra_status run_halpern(vajra_pdhg* h, vajra_result* r);
+
+// Closed forms for LPs without rows or without nonzeros (pdhg.cpp:88-127 for m = 0 / n = 0;
+// for nnz = 0 the rows decouple from the columns).  Returns true when it handled the LP.
+bool solve_trivial(const vajra_pdhg* h, vajra_result* r);
+
+void copy_out_vector(double* dst, const double* dev, int count, cudaStream_t st);
+
+}  // namespace vajra

@@ -1,0 +1,168 @@
+// Sparse matrix-vector kernels over CSR (A) and over the stored transpose (the CSC of A,
+// i.e. the CSR of A^T).  Each kernel hands every finished row sum to an epilogue functor,
+// which is where the dual / primal prox, Halpern and KKT work is fused, so a row sum never
+// makes a round trip through HBM.
+//
+// Two families:
+//   k_spmv_seq  one thread per row, products added in storage order with explicit _rn
+//               intrinsics (no FMA contraction).  Over a CSR whose rows are sorted by column
+//               this reproduces the reference's CSC scatter SpMV (src/linalg/sparse.cpp:196-217)
+//               and in-order dot (:219-238) bit for bit, including the |x_j| <= 1e-11 skip.
+//   k_spmv_vec  G lanes per row (G = 1..32, picked per matrix by the autotuner), coalesced
+//               strided loads with streaming (evict-first) cache hints for the matrix and
+//               cached gathers for the dense vector, xor-butterfly reduction (deterministic),
+//               and trailing CTAs that take the rows longer than `long_len` one CTA per row.
+#pragma once
+
+#include "common.cuh"
+
+namespace vajra {
+
+// ----- round-to-nearest arithmetic without contraction --------------------------------
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_div(float a, float b) { return __fdiv_rn(a, b); }
+
+template <typename T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+template <typename T> __device__ __forceinline__ T ld_cached(const T* p) { return __ldg(p); }
+
+// ----- the reference's elementwise updates, in its evaluation order --------------------
+// Dual Moreau step (src/solvers/pdhg/pdhg.cpp:204-209, spmv_kernels.cuh:173-178).
+template <typename T>
+__device__ __forceinline__ T dual_prox_exact(T y, T w, T sigma, T l, T u) {
+    const T y_hat = rn_add(y, rn_mul(sigma, w));
+    const T val = rn_div(y_hat, sigma);
+    const T clamped = (val < l) ? l : ((val > u) ? u : val);
+    return rn_sub(y_hat, rn_mul(sigma, clamped));
+}
+
+// Primal projected step (pdhg.cpp:229-235, spmv_kernels.cuh:197-202); returns x_new.
+template <typename T>
+__device__ __forceinline__ T primal_prox_exact(T x_old, T aty, T c, T tau, T l, T u) {
+    const T grad = rn_add(aty, c);
+    T x_new = rn_sub(x_old, rn_mul(tau, grad));
+    if (x_new < l) x_new = l;
+    if (x_new > u) x_new = u;
+    return x_new;
+}
+
+template <typename T>
+__device__ __forceinline__ T extrapolate_exact(T x_new, T x_old) {   // 2 x_new - x_old
+    return rn_sub(rn_mul(T(2), x_new), x_old);
+}
+
+// ----- epilogues usable by both families ---------------------------------------------
+template <typename T>
+struct EpiStore {
+    T* out;
+    __device__ bool active() const { return true; }
+    template <typename Acc> __device__ void operator()(int row, Acc s) const { out[row] = static_cast<T>(s); }
+};
+
+// ----- exact family -----------------------------------------------------------------
+// ZERO_DROP: skip products whose dense operand has |x_j| <= 1e-11, as the reference's CSC
+// multiply does (sparse.cpp:207).  Adding +0.0 instead of skipping is identical because a
+// sum that starts at +0.0 never becomes -0.0.
+template <typename V, bool ZERO_DROP, class Epi>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_seq(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+           const V* __restrict__ val, const V* __restrict__ x, Epi epi) {
+    if (!epi.active()) return;
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= rows) return;
+    const int64_t s = ptr[row], e = ptr[row + 1];
+    V sum = V(0);
+    for (int64_t k = s; k < e; ++k) {
+        const V xv = x[idx[k]];
+        if (ZERO_DROP && fabs(xv) <= V(kZeroDrop)) continue;
+        sum = rn_add(sum, rn_mul(val[k], xv));
+    }
+    epi(row, sum);
+}
+
+// ----- fast family --------------------------------------------------------------------
+template <typename V, typename Acc, int G, class Epi>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+           const V* __restrict__ val, const V* __restrict__ x, int64_t long_len,
+           const int32_t* __restrict__ long_rows, int vec_blocks, Epi epi) {
+    if (!epi.active()) return;
+    if (static_cast<int>(blockIdx.x) >= vec_blocks) {
+        // One CTA per long row.
+        __shared__ Acc red[32];
+        const int row = long_rows[blockIdx.x - vec_blocks];
+        const int64_t s = ptr[row], e = ptr[row + 1];
+        Acc acc = Acc(0);
+        for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+        Acc v[1] = {acc};
+        block_reduce<OpSum, Acc, 1>(v, red);
+        if (threadIdx.x == 0) epi(row, v[0]);
+        return;
+    }
+    const int lane = threadIdx.x & (G - 1);
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    bool valid = row < rows;
+    int64_t s = 0, e = 0;
+    if (valid) {
+        s = ptr[row];
+        e = ptr[row + 1];
+        if (e - s > long_len) valid = false;
+    }
+    Acc acc = Acc(0);
+    if (valid) {
+#pragma unroll 4
+        for (int64_t k = s + lane; k < e; k += G)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (valid && lane == 0) epi(row, acc);
+}
+
+// Host-side description of one SpMV operand (a CSR, possibly the stored transpose) and the
+// launch shape the autotuner chose for it.
+struct CsrView {
+    int rows = 0;
+    int cols = 0;
+    int64_t nnz = 0;
+    const int64_t* ptr = nullptr;
+    const int32_t* idx = nullptr;
+    int group = 8;                      // lanes per row (1,2,4,...,32)
+    int64_t long_len = 1 << 30;         // rows longer than this go one CTA per row
+    const int32_t* long_rows = nullptr; // device list of those rows
+    int n_long = 0;
+};
+
+template <typename V, typename Acc, int G, class Epi>
+inline void launch_vec_g(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
+    const int vec_blocks = static_cast<int>(grid_for(static_cast<int64_t>(a.rows) * G));
+    k_spmv_vec<V, Acc, G, Epi><<<vec_blocks + a.n_long, kThreads, 0, st>>>(
+        a.rows, a.ptr, a.idx, val, x, a.long_len, a.long_rows, vec_blocks, epi);
+}
+
+template <typename V, typename Acc, class Epi>
+inline void launch_spmv(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
+    if (a.rows <= 0) return;
+    switch (a.group) {
+        case 1: launch_vec_g<V, Acc, 1>(a, val, x, epi, st); break;
+        case 2: launch_vec_g<V, Acc, 2>(a, val, x, epi, st); break;
+        case 4: launch_vec_g<V, Acc, 4>(a, val, x, epi, st); break;
+        case 8: launch_vec_g<V, Acc, 8>(a, val, x, epi, st); break;
+        case 16: launch_vec_g<V, Acc, 16>(a, val, x, epi, st); break;
+        default: launch_vec_g<V, Acc, 32>(a, val, x, epi, st); break;
+    }
+}
+
+template <typename V, bool ZERO_DROP, class Epi>
+inline void launch_spmv_exact(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
+    if (a.rows <= 0) return;
+    k_spmv_seq<V, ZERO_DROP, Epi><<<grid_for(a.rows), kThreads, 0, st>>>(a.rows, a.ptr, a.idx, val, x, epi);
+}
+
+}  // namespace vajra
