@@ -15,14 +15,30 @@ pytestmark = pytest.mark.gpu
 KV = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "kernel_vectors.json")))
 
 
+_KEEP = []   # device tensors stay referenced until the test module ends
+
+
 def dev(a, dtype=None):
+    """Host array -> CUDA tensor that stays alive (a freed tensor's block would be reused by
+    the next allocation while the C call still holds its address)."""
     import torch
     a = np.ascontiguousarray(a if dtype is None else np.asarray(a, dtype=dtype))
-    return torch.from_numpy(a).cuda()
+    t = torch.from_numpy(a).cuda()
+    _KEEP.append(t)
+    return t
 
 
 def p(t):
+    assert any(t is k for k in _KEEP), "pass only tensors created by dev()"
     return C.c_void_p(t.data_ptr())
+
+
+@pytest.fixture(autouse=True)
+def _release():
+    yield
+    import torch
+    torch.cuda.synchronize()
+    _KEEP.clear()
 
 
 def host(t):
@@ -66,9 +82,8 @@ def test_dual_and_primal_prox_golden(cuda):
 
 
 def test_device_diagnostics_golden(cuda):
-    import torch
     k = KV["diagnostics"]
-    out = torch.zeros(6, dtype=torch.float64, device="cuda")   # 48-byte DeviceDiagnostics
+    out = dev(np.zeros(6))   # 48-byte DeviceDiagnostics
     args = [p(dev(k[n], np.float64)) for n in ("ax", "row_lower", "row_upper", "aty", "c", "x", "y", "col_lower", "col_upper")]
     assert _capi.lib().vajra_device_diagnostics_f64(2, 2, *args, p(out), None) == 0
     d = _capi.VajraDeviceDiagnostics.from_buffer_copy(host(out).tobytes())
