@@ -150,6 +150,17 @@ typedef struct vajra_result {
     int64_t host_device_transfers;
     int32_t spmv_group_a;       /* lanes per row chosen for A x      (0 = sequential)     */
     int32_t spmv_group_at;      /* lanes per row chosen for A^T y                          */
+    /* Live kernel timing (HALPERN): CUDA-event durations of the fused iteration kernels,
+     * sampled on the solve's stream once per check interval, for the precision that ran
+     * most iterations, with the algorithmic bytes one launch must move. */
+    double primal_kernel_us;    /* v = A^T y + primal prox / Halpern (stored transpose)   */
+    double dual_kernel_us;      /* w = A x_bar + dual prox / Halpern (CSR)                 */
+    double primal_kernel_bytes;
+    double dual_kernel_bytes;
+    int64_t kernel_samples;
+    int64_t kernel_launches;    /* kernels this solve launched (graph nodes counted per replay) */
+    double device_time_sec;     /* CUDA-event time on the solve's stream from the start of the
+                                   device set-up to the end of post-processing (no downloads) */
     char status_message[256];
 } vajra_result;
 

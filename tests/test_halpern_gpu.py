@@ -1,0 +1,137 @@
+"""VAJRA_ALGO_HALPERN (restarted reflected Halpern PDHG) on the device, FP64 and mixed:
+relative KKT <= 1e-6 verified independently in FP64 on the host, objective against the
+planted optimum / HiGHS, the reference's own KKT verifier, determinism and limits."""
+import numpy as np
+import pytest
+import scipy.optimize as so
+
+import vajra_pdhg as V
+from oracle import bindings as B
+from vajra_pdhg import workloads as W
+from vajra_pdhg.kkt import relative_kkt
+
+pytestmark = pytest.mark.gpu
+INF = 1e20
+PRECISIONS = [V.PREC_FP64, V.PREC_MIXED]
+
+
+def highs(lp):
+    A = lp.to_scipy_csc()
+    sign = -1.0 if lp.sense else 1.0
+    rl, ru = lp.row_lower, lp.row_upper
+    eq = (rl == ru)
+    A_ub, b_ub = [], []
+    import scipy.sparse as sp
+    up = (~eq) & (ru < INF)
+    lo = (~eq) & (rl > -INF)
+    A_ub = sp.vstack([A[up], -A[lo]]) if (up.any() or lo.any()) else None
+    b_ub = np.concatenate([ru[up], -rl[lo]]) if A_ub is not None else None
+    bounds = list(zip(np.where(lp.col_lower > -INF, lp.col_lower, None), np.where(lp.col_upper < INF, lp.col_upper, None)))
+    res = so.linprog(sign * lp.c, A_ub=A_ub, b_ub=b_ub, A_eq=A[eq] if eq.any() else None,
+                     b_eq=rl[eq] if eq.any() else None, bounds=bounds, method="highs")
+    assert res.status == 0, res.message
+    return sign * res.fun + lp.objective_offset
+
+
+def check_solution(lp, g, tol=1e-6, obj=None, obj_tol=1e-5):
+    assert g["status_name"] == "OPTIMAL", g["status_message"]
+    assert g["rel_kkt"] <= tol
+    k = relative_kkt(lp, g["x"], g["y"])
+    assert k["rel_kkt"] <= 1.05 * tol + 1e-12, k            # host FP64 check of the device figure
+    assert abs(k["rel_kkt"] - g["rel_kkt"]) <= 1e-8 + 1e-3 * g["rel_kkt"], (k, g["rel_kkt"])
+    assert abs(g["objective_value"] - k["primal_objective"] * (-1 if lp.sense else 1)) <= 1e-7 * (1 + abs(g["objective_value"]))
+    if obj is not None:
+        assert abs(g["objective_value"] - obj) <= obj_tol * (1 + abs(obj)), (g["objective_value"], obj)
+    np.testing.assert_allclose(g["row_value"], lp.to_scipy_csc() @ g["x"], rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("m,n,seed", [(200, 500, 0), (2000, 5000, 1)])
+def test_planted_optimum(cuda, prec, m, n, seed):
+    lp = W.random_planted(m, n, 8, seed=seed)
+    g = V.solve(lp, precision=prec)
+    check_solution(lp, g, obj=lp.planted_objective)
+    if B.ref_available():
+        v = B.ref_verify(lp, g["x"], g["y"], g["objective_value"], g["status"], tol=1e-4)
+        assert v["primal_feasible"] and v["objective_matches"], v["summary"]
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("seed", [3, 4])
+def test_mixed_senses_vs_highs(cuda, prec, seed):
+    lp = W.small_random(300, 700, seed)
+    g = V.solve(lp, precision=prec)
+    check_solution(lp, g, obj=highs(lp))
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_maximise_free_columns_vs_highs(cuda, prec):
+    lp = W.small_random(150, 400, 9)
+    lp.sense = 1
+    lp.c = -lp.c
+    lp.objective_offset = 3.5
+    lp.col_lower = lp.col_lower.copy(); lp.col_upper = lp.col_upper.copy()
+    lp.col_lower[::11] = -INF
+    g = V.solve(lp, precision=prec)
+    check_solution(lp, g, obj=highs(lp))
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_min_cost_flow_vs_highs(cuda, prec):
+    lp = W.min_cost_flow(nodes=2000, arcs=15000, seed=5)
+    g = V.solve(lp, precision=prec)
+    check_solution(lp, g, obj=highs(lp))
+
+
+PDHG_TEST_OPTIMA = [   # tests/test_pdhg.cpp LPs and optima
+    ((3, 2, [(0, 0, 1), (0, 1, 1), (1, 0, 1), (2, 1, 1)], [-1, -2], [0, 0], [INF, INF], [-INF] * 3, [4, 3, 3], 0), -7.0),
+    ((2, 3, [(0, 0, 1), (0, 1, 1), (0, 2, 1), (1, 0, 2), (1, 1, 1)], [1, 2, 3], [0] * 3, [INF] * 3, [6, 5], [6, 5], 0), 13.0),
+    ((3, 2, [(0, 0, 1), (0, 1, 1), (1, 0, 1), (1, 1, -1), (2, 0, 2), (2, 1, 1)], [2, 3], [0, 0], [10, 10],
+      [2, -INF, 1], [INF, 4, 6], 0), 4.0),
+    ((1, 2, [(0, 0, 1), (0, 1, 1)], [2, 1], [-10, -INF], [10, INF], [5], [5], 0), -5.0),
+    ((1, 2, [(0, 0, 1), (0, 1, 1)], [-2, -3], [0, 0], [INF, INF], [-INF], [5], 0), -15.0),
+    ((1, 2, [(0, 0, 1), (0, 1, 1)], [2, 3], [0, 0], [INF, INF], [-INF], [5], 1), 15.0),
+    ((1, 2, [(0, 0, 1), (0, 1, 1)], [1, 1], [0, 0], [10, 10], [3], [10], 0), 3.0),
+]
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+@pytest.mark.parametrize("case", range(len(PDHG_TEST_OPTIMA)))
+def test_reference_test_lps_reach_optimum(cuda, prec, case):
+    (m, n, trips, c, cl, cu, rl, ru, sense), opt = PDHG_TEST_OPTIMA[case]
+    cp, ri, vals = W.canonical_csc(m, n, [t[0] for t in trips], [t[1] for t in trips], [t[2] for t in trips])
+    lp = W.LP(m, n, cp, ri, vals, np.array(c, float), np.array(cl, float), np.array(cu, float), np.array(rl, float),
+              np.array(ru, float), sense=sense)
+    g = V.solve(lp, precision=prec)
+    check_solution(lp, g, obj=opt)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_deterministic(cuda, prec):
+    lp = W.random_planted(500, 1200, 6, seed=21)
+    with V.Solver(lp, precision=prec) as s:
+        a, b = s.run(), s.run()
+    for k in ("x", "y", "d", "row_value"):
+        np.testing.assert_array_equal(a[k], b[k])
+    assert a["iterations"] == b["iterations"] and a["rel_kkt"] == b["rel_kkt"]
+
+
+def test_iteration_limit_and_partial_chunk(cuda):
+    lp = W.random_planted(500, 1200, 6, seed=22)
+    g = V.solve(lp, precision=V.PREC_FP64, iteration_limit=100)
+    assert g["status_name"] == "ITERATION_LIMIT" and g["iterations"] == 100
+    g = V.solve(lp, precision=V.PREC_FP64, iteration_limit=0)
+    assert g["status_name"] == "ITERATION_LIMIT" and g["iterations"] == 0
+
+
+def test_nan_objective_is_numerical_error(cuda):
+    lp = W.random_planted(100, 250, 5, seed=23)
+    lp.c = lp.c.copy(); lp.c[3] = np.nan
+    g = V.solve(lp, precision=V.PREC_FP64)
+    assert g["status_name"] == "NUMERICAL_ERROR"
+
+
+def test_mixed_splits_iterations(cuda):
+    lp = W.random_planted(2000, 5000, 8, seed=24)
+    g = V.solve(lp, precision=V.PREC_MIXED)
+    assert g["fp32_iterations"] > 0 and g["fp32_iterations"] + g["fp64_iterations"] == g["iterations"]

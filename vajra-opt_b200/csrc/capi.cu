@@ -15,7 +15,10 @@ namespace vajra {
 namespace {
 thread_local char g_error[512] = "";
 thread_local vajra_timing g_last_timing = {};
+thread_local int64_t g_launches = 0;
 }  // namespace
+
+int64_t& launch_count() { return g_launches; }
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -315,6 +318,7 @@ vajra_status vajra_pdhg_run(vajra_pdhg* h, vajra_result* r) {
     r->status = VAJRA_SOLVE_NOT_SOLVED;
     r->status_message[0] = '\0';
     vajra_status s = VAJRA_OK;
+    const int64_t launches0 = launch_count();
     if (cudaSetDevice(h->device) != cudaSuccess) {
         s = cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__);
     } else if (solve_trivial(h, r)) {
@@ -331,6 +335,7 @@ vajra_status vajra_pdhg_run(vajra_pdhg* h, vajra_result* r) {
         cudaGetLastError();
         if (h->stream) cudaStreamSynchronize(h->stream);
     }
+    r->kernel_launches = launch_count() - launches0;
     r->upload_time_sec = h->upload_time_sec;
     r->total_time_sec = seconds_since(t0) + h->upload_time_sec;
     r->host_device_transfers = h->transfers;

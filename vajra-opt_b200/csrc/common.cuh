@@ -17,6 +17,10 @@ namespace vajra {
 void set_error(const char* fmt, ...);
 const char* last_error();
 
+// Kernels launched by the calling thread (graph replays count every captured node).
+int64_t& launch_count();
+inline void note_launch(int64_t k = 1) { launch_count() += k; }
+
 vajra_status cuda_status(cudaError_t e, const char* what, const char* file, int line);
 
 #define VJ_CUDA(call)                                                                  \

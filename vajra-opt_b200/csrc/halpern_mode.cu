@@ -1,10 +1,769 @@
-// VAJRA_ALGO_HALPERN (placeholder until the restarted Halpern driver lands).
+// VAJRA_ALGO_HALPERN: restarted reflected Halpern PDHG with KKT-driven adaptive restarts and
+// primal-weight updates, terminated on the FP64 relative KKT error of the original LP.
+//
+// Operator T (primal first; same saddle form as the reference, pdhg.cpp:196-241):
+//   x+ = proj_X(x - tau (c + A^T y)),   y+ = prox_{sigma h*}(y + sigma A (2 x+ - x))
+// Halpern step with reflection gamma, inner index k since the last restart, anchor z0:
+//   z_{k+1} = (k+1)/(k+2) ((1+gamma) T(z_k) - gamma z_k) + 1/(k+2) z0
+// Two fused kernels per iteration:
+//   primal: v = A^T y over the stored transpose -> x+, x_bar = 2x+ - x, x <- Halpern
+//   dual  : w = A x_bar over CSR                -> y+, y <- Halpern
+// Every check_frequency iterations (the chunk, captured once as a CUDA graph) the candidate
+// T(z) is evaluated in FP64 with FP64 matrix values: A x+, A^T y+, then row / column passes
+// with deterministic block partials and one control CTA that forms the relative KKT on the
+// original problem, the primal-weighted KKT for restarts (sufficient 0.2 / necessary 0.8 +
+// no progress / artificial 0.36 of total), the primal-weight update at restarts, and -- in
+// mixed precision -- the hand-over from the FP32 phase to the FP64 polish.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "solver.cuh"
 
 namespace vajra {
-vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
-    (void)h; (void)r;
-    set_error("HALPERN driver not built yet");
-    return VAJRA_ERR_INTERNAL;
+namespace {
+
+constexpr int kQ = 6;             // partial sums per block in the check passes
+constexpr int kCheckBlocks = 148 * 4;
+constexpr int kHist = 16;
+
+struct HState {
+    double omega, eta, tau, sigma;
+    double kkt_start, kkt_prev;
+    double rel_p, rel_d, rel_gap, rel_kkt, pobj, dobj;
+    double bnorm, cnorm, offset_min;
+    double hist[kHist];
+    long long k_base;
+    long long total;
+    long long phase_iters[2];
+    long long stop_iter;
+    int hist_n;
+    int phase;          // 0: FP32 phase of the mixed mode, 1: FP64
+    int stop;
+    int status;
+    int restart_count;
+    int restart_flag;
+    int switch_flag;
+    int pad;
+};
+
+constexpr int kStatusOptimal = 1;
+constexpr int kStatusIterLimit = 6;
+constexpr int kStatusTimeLimit = 7;
+constexpr int kStatusNumerical = 9;
+
+template <typename T>
+struct EpiHPrimal {
+    const T* c; const T* cl; const T* cu; const T* x0;
+    T* x; T* xb; T* xc;
+    const HState* st;
+    double gamma;
+    int kk, phase, write_cand;
+    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
+    template <typename Acc>
+    __device__ void operator()(int j, Acc v) const {
+        const double k = static_cast<double>(st->k_base + kk);
+        const T w1 = static_cast<T>((k + 1.0) / (k + 2.0));
+        const T w0 = static_cast<T>(1.0 / (k + 2.0));
+        const T tau = static_cast<T>(st->tau);
+        const T g = static_cast<T>(gamma);
+        const T xo = x[j];
+        T xp = xo - tau * (c[j] + static_cast<T>(v));
+        xp = xp < cl[j] ? cl[j] : (xp > cu[j] ? cu[j] : xp);
+        xb[j] = xp + xp - xo;
+        x[j] = w1 * ((T(1) + g) * xp - g * xo) + w0 * x0[j];
+        if (write_cand) xc[j] = xp;
+    }
+};
+
+template <typename T>
+struct EpiHDual {
+    const T* rl; const T* ru; const T* y0;
+    T* y; T* yc;
+    const HState* st;
+    double gamma;
+    int kk, phase, write_cand;
+    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
+    template <typename Acc>
+    __device__ void operator()(int i, Acc w) const {
+        const double k = static_cast<double>(st->k_base + kk);
+        const T w1 = static_cast<T>((k + 1.0) / (k + 2.0));
+        const T w0 = static_cast<T>(1.0 / (k + 2.0));
+        const T sigma = static_cast<T>(st->sigma);
+        const T g = static_cast<T>(gamma);
+        const T yo = y[i];
+        const T yh = yo + sigma * static_cast<T>(w);
+        T q = yh / sigma;
+        q = q < rl[i] ? rl[i] : (q > ru[i] ? ru[i] : q);
+        const T yp = yh - sigma * q;
+        y[i] = w1 * ((T(1) + g) * yp - g * yo) + w0 * y0[i];
+        if (write_cand) yc[i] = yp;
+    }
+};
+
+struct EpiStoreActive {
+    double* out;
+    const HState* st;
+    int phase;
+    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
+    template <typename Acc> __device__ void operator()(int i, Acc s) const { out[i] = static_cast<double>(s); }
+};
+
+__device__ __forceinline__ bool finite_lo(double l) { return l > -1e20; }
+__device__ __forceinline__ bool finite_up(double u) { return u < 1e20; }
+
+// Row pass: original- and scaled-space primal residual, row part of the dual objective,
+// distance of y+ from the last restart point, NaN detection.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const double* __restrict__ rl_s,
+           const double* __restrict__ ru_s, const double* __restrict__ rl_o, const double* __restrict__ ru_o,
+           const double* __restrict__ rs, const double* __restrict__ y_last, double* __restrict__ part,
+           const HState* st, int phase) {
+    if (st->stop || st->phase != phase) return;
+    __shared__ double red[kQ * 32];
+    double v[kQ] = {0, 0, 0, 0, 0, 0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const double a = ax[i];
+        const double ys = static_cast<double>(yc[i]);
+        if (!isfinite(a) || !isfinite(ys)) v[5] = 1.0;
+        const double ps = a - fmin(fmax(a, rl_s[i]), ru_s[i]);
+        const double ao = a / rs[i];
+        const double po = ao - fmin(fmax(ao, rl_o[i]), ru_o[i]);
+        const double yo = -ys * rs[i];          // verifier sign, original space
+        double dt = 0.0;
+        if (yo > 0.0 && finite_lo(rl_o[i])) dt = yo * rl_o[i];
+        else if (yo < 0.0 && finite_up(ru_o[i])) dt = yo * ru_o[i];
+        const double dy = ys - y_last[i];
+        v[0] += po * po;
+        v[1] += ps * ps;
+        v[2] += dt;
+        v[3] += dy * dy;
+    }
+    block_reduce<OpSum, double, kQ - 1>(*reinterpret_cast<double(*)[kQ - 1]>(v), red);
+    double f[1] = {v[5]};
+    block_reduce<OpMax, double, 1>(f, red);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kQ - 1; ++q) part[blockIdx.x * kQ + q] = v[q];
+        part[blockIdx.x * kQ + kQ - 1] = f[0];
+    }
 }
+
+// Column pass: reduced cost r = c + A^T y (min form), its bound-multiplier part lambda,
+// dual residual r - lambda (original and scaled), primal objective, column part of the dual
+// objective, distance of x+ from the last restart point.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_kkt_cols(int n, const double* __restrict__ aty, const T* __restrict__ xc, const double* __restrict__ c_s,
+           const double* __restrict__ cl_o, const double* __restrict__ cu_o, const double* __restrict__ cs,
+           const double* __restrict__ x_last, double* __restrict__ part, const HState* st, int phase) {
+    if (st->stop || st->phase != phase) return;
+    __shared__ double red[kQ * 32];
+    double v[kQ] = {0, 0, 0, 0, 0, 0};   // rd_o^2, rd_s^2, pobj, dobj, dx^2, nan
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const double at = aty[j];
+        const double xs = static_cast<double>(xc[j]);
+        if (!isfinite(at) || !isfinite(xs)) v[5] = 1.0;
+        const bool lf = finite_lo(cl_o[j]), uf = finite_up(cu_o[j]);
+        const double r_s = c_s[j] + at;
+        const double r_o = r_s / cs[j];
+        auto lam_of = [&](double r) { return (lf && uf) ? r : lf ? fmax(r, 0.0) : uf ? fmin(r, 0.0) : 0.0; };
+        const double lo = lam_of(r_o), ls = lam_of(r_s);
+        const double ro = r_o - lo, rsd = r_s - ls;
+        double dt = 0.0;
+        if (lo > 0.0) dt = lo * cl_o[j];
+        else if (lo < 0.0) dt = lo * cu_o[j];
+        const double dx = xs - x_last[j];
+        v[0] += ro * ro;
+        v[1] += rsd * rsd;
+        v[2] += c_s[j] * xs;
+        v[3] += dt;
+        v[4] += dx * dx;
+    }
+    block_reduce<OpSum, double, kQ - 1>(*reinterpret_cast<double(*)[kQ - 1]>(v), red);
+    double f[1] = {v[5]};
+    block_reduce<OpMax, double, 1>(f, red);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kQ - 1; ++q) part[blockIdx.x * kQ + q] = v[q];
+        part[blockIdx.x * kQ + kQ - 1] = f[0];
+    }
+}
+
+struct ControlParams {
+    double tol;
+    double switch_tol;
+    double beta_sufficient;
+    double beta_necessary;
+    double beta_artificial;
+    double pw_smoothing;
+    int len;          // iterations in the chunk just finished
+    int phase;
+    int mixed;        // 1 when an FP32 phase hands over to FP64
+};
+
+__global__ void __launch_bounds__(1024)
+k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ part_c, ControlParams cp,
+                  HState* st) {
+    if (st->stop || st->phase != cp.phase) return;
+    __shared__ double red[10 * 32];
+    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x) {
+        for (int q = 0; q < kQ - 1; ++q) { s[q] += part_r[b * kQ + q]; s[5 + q] += part_c[b * kQ + q]; }
+    }
+    block_reduce<OpSum, double, 10>(s, red);
+    double f[1] = {0.0};
+    for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x)
+        f[0] = fmax(f[0], fmax(part_r[b * kQ + kQ - 1], part_c[b * kQ + kQ - 1]));
+    block_reduce<OpMax, double, 1>(f, red);
+    if (threadIdx.x != 0) return;
+    const double rp_o2 = s[0], rp_s2 = s[1], dobj_r = s[2], dy2 = s[3];
+    const double rd_o2 = s[5], rd_s2 = s[6], pobj_s = s[7], dobj_c = s[8], dx2 = s[9];
+    st->total += cp.len;
+    st->phase_iters[cp.phase] += cp.len;
+    st->restart_flag = 0;
+    st->switch_flag = 0;
+    if (f[0] > 0.0 || isnan(rp_o2) || isnan(rd_o2)) {
+        st->stop = 1;
+        st->status = kStatusNumerical;
+        st->stop_iter = st->total;
+        return;
+    }
+    const double pobj = pobj_s + st->offset_min;
+    const double dobj = dobj_r + dobj_c + st->offset_min;
+    const double rel_p = sqrt(rp_o2) / (1.0 + st->bnorm);
+    const double rel_d = sqrt(rd_o2) / (1.0 + st->cnorm);
+    const double rel_gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    const double rel = fmax(rel_p, fmax(rel_d, rel_gap));
+    st->rel_p = rel_p; st->rel_d = rel_d; st->rel_gap = rel_gap; st->rel_kkt = rel;
+    st->pobj = pobj; st->dobj = dobj;
+    if (rel <= cp.tol) {
+        st->stop = 1;
+        st->status = kStatusOptimal;
+        st->stop_iter = st->total;
+        return;
+    }
+    const double omega = st->omega;
+    const double wk = sqrt(omega * rp_s2 + rd_s2 / omega + rel_gap * rel_gap);
+    if (cp.mixed && cp.phase == 0) {
+        const int hn = st->hist_n;
+        bool stalled = false;
+        if (hn >= 10) {
+            const double old = st->hist[(hn - 10) % kHist];
+            stalled = rel > 0.95 * old;
+        }
+        st->hist[hn % kHist] = rel;
+        st->hist_n = hn + 1;
+        if (rel <= cp.switch_tol || stalled) {
+            st->switch_flag = 1;
+            st->phase = 1;
+            st->k_base = 0;
+            st->kkt_start = wk;
+            st->kkt_prev = wk;
+            return;
+        }
+    }
+    if (st->kkt_start < 0.0) { st->kkt_start = wk; st->kkt_prev = wk; }
+    const long long k_in = st->k_base + cp.len;
+    const bool restart = (wk <= cp.beta_sufficient * st->kkt_start) ||
+                         (wk <= cp.beta_necessary * st->kkt_start && wk > st->kkt_prev) ||
+                         (static_cast<double>(k_in) >= cp.beta_artificial * static_cast<double>(st->total));
+    st->kkt_prev = wk;
+    if (restart) {
+        const double dx = sqrt(dx2), dy = sqrt(dy2);
+        if (dx > 1e-10 && dy > 1e-10) {
+            const double th = cp.pw_smoothing;
+            st->omega = exp(th * log(dy / dx) + (1.0 - th) * log(omega));
+            st->tau = st->eta / st->omega;
+            st->sigma = st->eta * st->omega;
+        }
+        st->k_base = 0;
+        st->kkt_start = wk;
+        st->kkt_prev = wk;
+        st->restart_count += 1;
+        st->restart_flag = 1;
+    } else {
+        st->k_base = k_in;
+    }
+}
+
+template <typename T>
+__global__ void k_halpern_restart(int m, int n, const T* __restrict__ xc, const T* __restrict__ yc, T* __restrict__ x,
+                                  T* __restrict__ x0, T* __restrict__ y, T* __restrict__ y0, double* __restrict__ x_last,
+                                  double* __restrict__ y_last, const HState* st) {
+    if (!st->restart_flag) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { const T v = xc[i]; x[i] = v; x0[i] = v; x_last[i] = static_cast<double>(v); }
+    if (i < m) { const T v = yc[i]; y[i] = v; y0[i] = v; y_last[i] = static_cast<double>(v); }
+}
+
+// FP32 -> FP64 hand-over: the FP32 candidate becomes the FP64 iterate and anchor.
+__global__ void k_handover(int m, int n, const float* __restrict__ xc32, const float* __restrict__ yc32,
+                           double* __restrict__ x, double* __restrict__ x0, double* __restrict__ xc,
+                           double* __restrict__ y, double* __restrict__ y0, double* __restrict__ yc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { const double v = xc32[i]; x[i] = v; x0[i] = v; xc[i] = v; }
+    if (i < m) { const double v = yc32[i]; y[i] = v; y0[i] = v; yc[i] = v; }
+}
+
+template <typename T>
+__global__ void k_init_iterates(int m, int n, const double* __restrict__ cl, const double* __restrict__ cu,
+                                T* __restrict__ x, T* __restrict__ x0, T* __restrict__ xb, T* __restrict__ xc,
+                                T* __restrict__ y, T* __restrict__ y0, T* __restrict__ yc,
+                                double* __restrict__ x_last, double* __restrict__ y_last) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double v = fmin(fmax(0.0, cl[i]), cu[i]);
+        x[i] = x0[i] = xb[i] = xc[i] = static_cast<T>(v);
+        x_last[i] = static_cast<double>(static_cast<T>(v));
+    }
+    if (i < m) { y[i] = y0[i] = yc[i] = T(0); y_last[i] = 0.0; }
+}
+
+template <typename T>
+__global__ void k_to_t(int64_t n, const double* __restrict__ s, T* __restrict__ d) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        d[k] = static_cast<T>(s[k]);
+}
+
+// ||b|| (finite row bounds, each equality row once), ||c||, scaled ||b||, ||c|| for the
+// initial primal weight.
+__global__ void __launch_bounds__(1024)
+k_norms(int m, int n, const double* __restrict__ rl_o, const double* __restrict__ ru_o, const double* __restrict__ c_o,
+        const double* __restrict__ rl_s, const double* __restrict__ ru_s, const double* __restrict__ c_s,
+        double* __restrict__ out) {
+    __shared__ double red[4 * 32];
+    double v[4] = {0, 0, 0, 0};
+    auto b2 = [](double l, double u) {
+        const bool lf = l > -1e20, uf = u < 1e20;
+        if (lf && uf && l == u) return l * l;
+        return (lf ? l * l : 0.0) + (uf ? u * u : 0.0);
+    };
+    for (int i = threadIdx.x; i < m; i += blockDim.x) { v[0] += b2(rl_o[i], ru_o[i]); v[2] += b2(rl_s[i], ru_s[i]); }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) { v[1] += c_o[j] * c_o[j]; v[3] += c_s[j] * c_s[j]; }
+    block_reduce<OpSum, double, 4>(v, red);
+    if (threadIdx.x == 0) for (int q = 0; q < 4; ++q) out[q] = sqrt(v[q]);
+}
+
+__global__ void k_post_vectors(int m, int n, const double* __restrict__ xc, const double* __restrict__ yc,
+                               const double* __restrict__ cs, const double* __restrict__ rs, int scaled, int is_max,
+                               double* __restrict__ x_out, double* __restrict__ y_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x_out[i] = scaled ? xc[i] * cs[i] : xc[i];
+    if (i < m) { const double v = scaled ? yc[i] * rs[i] : yc[i]; y_out[i] = is_max ? v : -v; }
+}
+
+template <typename T>
+__global__ void k_widen(int k, const T* __restrict__ s, double* __restrict__ d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) d[i] = static_cast<double>(s[i]);
+}
+
+__global__ void __launch_bounds__(1024)
+k_dot_offset(int n, const double* __restrict__ a, const double* __restrict__ b, double offset, double* out) {
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    for (int j = threadIdx.x; j < n; j += blockDim.x) v[0] += a[j] * b[j];
+    block_reduce<OpSum, double, 1>(v, red);
+    if (threadIdx.x == 0) *out = offset + v[0];
+}
+
+__global__ void k_sub_from(int n, const double* __restrict__ c, double* __restrict__ d) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) d[j] = c[j] - d[j];
+}
+
+// One precision's iterate set, kernels and captured chunk graph.
+template <typename T>
+struct Phase {
+    int m = 0, n = 0, phase = 0;
+    DeviceBuffer<T> x, x0, xb, xc, y, y0, yc;
+    DeviceBuffer<T> c, cl, cu, rl, ru;          // iteration copies in T (FP64: separate copies too)
+    const T* csr_val = nullptr;
+    const T* csc_val = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // around the first iteration of a chunk
+    double t_primal_ms = 0.0, t_dual_ms = 0.0;
+    int64_t samples = 0;
+    int64_t graph_kernels = 0;   // kernels captured in one chunk graph
+    ~Phase() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto& e : ev) if (e) cudaEventDestroy(e);
+    }
+    vajra_status alloc(int m_, int n_, const Prepared& p, cudaStream_t st) {
+        m = m_; n = n_;
+        for (auto& e : ev) VJ_CUDA(cudaEventCreate(&e));
+        for (auto* b : {&x, &x0, &xb, &xc, &c, &cl, &cu}) VJ_TRY(b->alloc(n));
+        for (auto* b : {&y, &y0, &yc, &rl, &ru}) VJ_TRY(b->alloc(m));
+        const unsigned gn = grid_for(n, kThreads, 148 * 32), gm = grid_for(m, kThreads, 148 * 32);
+        k_to_t<T><<<gn, kThreads, 0, st>>>(n, p.c.get(), c.get());
+        k_to_t<T><<<gn, kThreads, 0, st>>>(n, p.col_lower.get(), cl.get());
+        k_to_t<T><<<gn, kThreads, 0, st>>>(n, p.col_upper.get(), cu.get());
+        k_to_t<T><<<gm, kThreads, 0, st>>>(m, p.row_lower.get(), rl.get());
+        k_to_t<T><<<gm, kThreads, 0, st>>>(m, p.row_upper.get(), ru.get());
+        VJ_LAUNCH_CHECK();
+        note_launch(5);
+        return VAJRA_OK;
+    }
+};
+
+// `timed`: bracket the two kernels with event-record nodes (captured into the chunk graph).
+template <typename T>
+void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, double gamma, int kk,
+                       int write_cand, bool timed, cudaStream_t st) {
+    if (timed) cudaEventRecordWithFlags(ph.ev[0], st, cudaEventRecordExternal);
+    launch_spmv_t<T, T, T>(at, ph.csc_val, ph.y.get(),
+                           EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
+                                         ph.xc.get(), S, gamma, kk, ph.phase, write_cand}, st);
+    if (timed) cudaEventRecordWithFlags(ph.ev[1], st, cudaEventRecordExternal);
+    launch_spmv_t<T, T, T>(a, ph.csr_val, ph.xb.get(),
+                           EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), S, gamma, kk,
+                                       ph.phase, write_cand}, st);
+    if (timed) cudaEventRecordWithFlags(ph.ev[2], st, cudaEventRecordExternal);
+}
+
+struct CheckBuffers {
+    DeviceBuffer<double> ax, aty, part_r, part_c, x_last, y_last;
+};
+
+template <typename T>
+void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const Prepared& p, const DeviceLp& lp,
+                   CheckBuffers& cb, HState* S, const ControlParams& cp, cudaStream_t st) {
+    launch_spmv_t<double, T, double>(a64, p.csr_val.get(), ph.xc.get(), EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
+    launch_spmv_t<double, T, double>(at64, p.csc_val.get(), ph.yc.get(), EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
+    k_kkt_rows<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.m, cb.ax.get(), ph.yc.get(), p.row_lower.get(), p.row_upper.get(),
+                                                     lp.row_lower.get(), lp.row_upper.get(), p.row_scale.get(),
+                                                     cb.y_last.get(), cb.part_r.get(), S, ph.phase);
+    k_kkt_cols<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.n, cb.aty.get(), ph.xc.get(), p.c.get(), lp.col_lower.get(),
+                                                     lp.col_upper.get(), p.col_scale.get(), cb.x_last.get(),
+                                                     cb.part_c.get(), S, ph.phase);
+    k_halpern_control<<<1, 1024, 0, st>>>(cb.part_r.get(), cb.part_c.get(), cp, S);
+    const int mx = ph.m > ph.n ? ph.m : ph.n;
+    k_halpern_restart<T><<<grid_for(mx), kThreads, 0, st>>>(ph.m, ph.n, ph.xc.get(), ph.yc.get(), ph.x.get(),
+                                                            ph.x0.get(), ph.y.get(), ph.y0.get(), cb.x_last.get(),
+                                                            cb.y_last.get(), S);
+    note_launch(4);
+}
+
+template <typename T>
+void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrView& a64, const CsrView& at64,
+                   const Prepared& p, const DeviceLp& lp, CheckBuffers& cb, HState* S, double gamma, int len,
+                   ControlParams cp, cudaStream_t st) {
+    for (int kk = 0; kk < len; ++kk)
+        enqueue_iteration(ph, a, at, S, gamma, kk, kk == len - 1 ? 1 : 0, kk == 0 && len > 1, st);
+    cp.len = len;
+    cp.phase = ph.phase;
+    enqueue_check(ph, a64, at64, p, lp, cb, S, cp, st);
+}
+
+// Times every lane-group size of one SpMV (store epilogue) and keeps the fastest.
+template <typename T>
+vajra_status autotune(CsrView& v, const T* val, const T* xin, T* out, cudaStream_t st) {
+    if (v.rows <= 0) return VAJRA_OK;
+    cudaEvent_t e0, e1;
+    VJ_CUDA(cudaEventCreate(&e0));
+    VJ_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_g = v.group;
+    for (int g : {1, 2, 4, 8, 16, 32}) {
+        CsrView t = v;
+        t.group = g;
+        launch_spmv_t<T, T, T>(t, val, xin, EpiStore<T>{out}, st);     // warm
+        VJ_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < 3; ++r) launch_spmv_t<T, T, T>(t, val, xin, EpiStore<T>{out}, st);
+        VJ_CUDA(cudaEventRecord(e1, st));
+        VJ_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        VJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) { best = ms; best_g = g; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    v.group = best_g;
+    return VAJRA_OK;
+}
+
+}  // namespace
+
+vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
+    const auto t_start = Clock::now();
+    cudaStream_t st = h->stream;
+    StreamTimer dev_timer;
+    dev_timer.start(st);
+    const vajra_opts& o = h->opts;
+    const int m = h->m, n = h->n;
+    const int64_t nnz = h->nnz;
+    const bool is_max = h->sense != 0;
+    const bool mixed = o.precision == VAJRA_PREC_MIXED;
+    const DeviceLp& lp = h->lp;
+
+    Prepared p;
+    DeviceBuffer<SetupState> sst;
+    VJ_TRY(sst.alloc(1));
+    VJ_TRY(build_csr(lp, p, st));
+    ScalingOpts so;
+    so.enable = o.enable_scaling != 0;
+    so.ruiz_iterations = o.ruiz_iterations > 0 ? o.ruiz_iterations : 10;
+    so.ruiz_tolerance = 0.05;
+    so.pock_chambolle = o.pock_chambolle != 0;
+    so.negate_c = is_max;
+    VJ_TRY(prepare_scaled(lp, p, so, sst.get(), st));
+    VJ_TRY(plan_spmv(lp, p, st));
+    VJ_TRY(spectral_norm_fast(p, m, n, 100, 1e-5, sst.get(), st));
+    SetupState hss{};
+    VJ_CUDA(cudaMemcpy(&hss, sst.get(), sizeof(hss), cudaMemcpyDeviceToHost));
+    const double spectral_norm = hss.spectral_norm;
+    if (!(spectral_norm > 1e-12) || !std::isfinite(spectral_norm)) {
+        r->status = kStatusNumerical;
+        std::snprintf(r->status_message, sizeof(r->status_message), "invalid spectral norm estimate %g", spectral_norm);
+        return VAJRA_OK;
+    }
+    if (mixed) VJ_TRY(make_f32_values(p, nnz, st));
+
+    // Norms for the relative KKT and the initial primal weight.
+    DeviceBuffer<double> norms;
+    VJ_TRY(norms.alloc(4));
+    k_norms<<<1, 1024, 0, st>>>(m, n, lp.row_lower.get(), lp.row_upper.get(), lp.c.get(), p.row_lower.get(),
+                               p.row_upper.get(), p.c.get(), norms.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
+    double hn[4];
+    VJ_CUDA(cudaMemcpyAsync(hn, norms.get(), sizeof(hn), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+
+    Phase<float> p32;
+    Phase<double> p64;
+    p32.phase = 0;
+    p64.phase = 1;
+    if (mixed) {
+        VJ_TRY(p32.alloc(m, n, p, st));
+        p32.csr_val = p.csr_val32.get();
+        p32.csc_val = p.csc_val32.get();
+    }
+    VJ_TRY(p64.alloc(m, n, p, st));
+    p64.csr_val = p.csr_val.get();
+    p64.csc_val = p.csc_val.get();
+
+    CheckBuffers cb;
+    VJ_TRY(cb.ax.alloc(m));
+    VJ_TRY(cb.aty.alloc(n));
+    VJ_TRY(cb.part_r.alloc(kCheckBlocks * kQ));
+    VJ_TRY(cb.part_c.alloc(kCheckBlocks * kQ));
+    VJ_TRY(cb.x_last.alloc(n));
+    VJ_TRY(cb.y_last.alloc(m));
+
+    // Launch shapes: FP64 views for the checks, autotuned views for the iteration precision.
+    CsrView a64 = p.a, at64 = p.at;
+    CsrView a_it = p.a, at_it = p.at;
+    if (o.autotune) {
+        if (mixed) {
+            VJ_TRY(autotune<float>(a_it, p.csr_val32.get(), p32.xb.get(), p32.yc.get(), st));
+            VJ_TRY(autotune<float>(at_it, p.csc_val32.get(), p32.y.get(), p32.xc.get(), st));
+        } else {
+            VJ_TRY(autotune<double>(a_it, p.csr_val.get(), p64.xb.get(), p64.yc.get(), st));
+            VJ_TRY(autotune<double>(at_it, p.csc_val.get(), p64.y.get(), p64.xc.get(), st));
+        }
+        a64.group = a_it.group;
+        at64.group = at_it.group;
+    }
+
+    const int mx = m > n ? m : n;
+    if (mixed)
+        k_init_iterates<float><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), p32.x.get(),
+                                                                 p32.x0.get(), p32.xb.get(), p32.xc.get(), p32.y.get(),
+                                                                 p32.y0.get(), p32.yc.get(), cb.x_last.get(), cb.y_last.get());
+    else
+        k_init_iterates<double><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), p64.x.get(),
+                                                                  p64.x0.get(), p64.xb.get(), p64.xc.get(), p64.y.get(),
+                                                                  p64.y0.get(), p64.yc.get(), cb.x_last.get(), cb.y_last.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
+
+    HState init{};
+    const double eta = 0.99 / spectral_norm;
+    init.omega = (hn[2] > 1e-10 && hn[3] > 1e-10) ? hn[3] / hn[2] : 1.0;
+    init.eta = eta;
+    init.tau = eta / init.omega;
+    init.sigma = eta * init.omega;
+    init.kkt_start = -1.0;
+    init.kkt_prev = -1.0;
+    init.bnorm = hn[0];
+    init.cnorm = hn[1];
+    init.offset_min = is_max ? -h->objective_offset : h->objective_offset;
+    init.phase = mixed ? 0 : 1;
+    init.rel_kkt = 1e30;
+    DeviceBuffer<HState> dstate;
+    VJ_TRY(dstate.alloc(1));
+    VJ_CUDA(cudaMemcpyAsync(dstate.get(), &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    const double setup_time = seconds_since(t_start);
+
+    HState* S = dstate.get();
+    HState* hs = nullptr;
+    VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hs), sizeof(HState)));
+    struct PinnedFree { HState* p; ~PinnedFree() { if (p) cudaFreeHost(p); } } pin_guard{hs};
+
+    ControlParams cp{};
+    cp.tol = o.tolerance;
+    cp.switch_tol = o.mixed_switch_tolerance;
+    cp.beta_sufficient = 0.2;
+    cp.beta_necessary = 0.8;
+    cp.beta_artificial = 0.36;
+    cp.pw_smoothing = 0.5;
+    cp.mixed = mixed ? 1 : 0;
+    const double gamma = o.reflection;
+    const int K = o.check_frequency > 0 ? o.check_frequency : 64;
+    const int64_t max_iter = o.iteration_limit;
+
+    const auto t_iter = Clock::now();
+    int64_t launched = 0;
+    int cur_phase = mixed ? 0 : 1;
+    int timed_out = 0;
+    while (launched < max_iter) {
+        const int64_t remaining = max_iter - launched;
+        const int len = static_cast<int>(remaining < K ? remaining : K);
+        auto run_chunk = [&](auto& ph) -> vajra_status {
+            if (len == K) {
+                if (!ph.exec) {
+                    const int64_t before = launch_count();
+                    VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                    enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, st);
+                    VJ_CUDA(cudaStreamEndCapture(st, &ph.graph));
+                    VJ_CUDA(cudaGraphInstantiate(&ph.exec, ph.graph, 0));
+                    ph.graph_kernels = launch_count() - before;
+                    launch_count() = before;
+                }
+                VJ_CUDA(cudaGraphLaunch(ph.exec, st));
+                note_launch(ph.graph_kernels);
+            } else {
+                enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, st);
+                VJ_LAUNCH_CHECK();
+            }
+            return VAJRA_OK;
+        };
+        if (cur_phase == 0) { VJ_TRY(run_chunk(p32)); } else { VJ_TRY(run_chunk(p64)); }
+        launched += len;
+        VJ_CUDA(cudaMemcpyAsync(hs, S, sizeof(HState), cudaMemcpyDeviceToHost, st));
+        VJ_CUDA(cudaStreamSynchronize(st));
+        h->transfers++;
+        // Kernel durations of this chunk's first iteration, unless that phase had stopped
+        // working before the chunk began (then its kernels returned at once).
+        if (len > 1 && (hs->phase == cur_phase || hs->switch_flag) &&
+            !(hs->stop && hs->stop_iter < launched - len + 1)) {
+            float t01 = 0.f, t12 = 0.f;
+            cudaEvent_t* ev = cur_phase == 0 ? p32.ev : p64.ev;
+            if (cudaEventElapsedTime(&t01, ev[0], ev[1]) == cudaSuccess &&
+                cudaEventElapsedTime(&t12, ev[1], ev[2]) == cudaSuccess) {
+                auto& ph_t = cur_phase == 0 ? p32.t_primal_ms : p64.t_primal_ms;
+                auto& ph_d = cur_phase == 0 ? p32.t_dual_ms : p64.t_dual_ms;
+                auto& ph_n = cur_phase == 0 ? p32.samples : p64.samples;
+                ph_t += t01;
+                ph_d += t12;
+                ph_n += 1;
+            }
+            cudaGetLastError();
+        }
+        if (hs->stop) break;
+        if (hs->phase != cur_phase) {
+            k_handover<<<grid_for(mx), kThreads, 0, st>>>(m, n, p32.xc.get(), p32.yc.get(), p64.x.get(), p64.x0.get(),
+                                                          p64.xc.get(), p64.y.get(), p64.y0.get(), p64.yc.get());
+            VJ_LAUNCH_CHECK();
+            note_launch(1);
+            cur_phase = hs->phase;
+        }
+        if (seconds_since(t_start) > o.time_limit) { timed_out = 1; break; }
+    }
+    const double iter_time = seconds_since(t_iter);
+
+    // The returned point is the last evaluated candidate T(z) of the active precision.
+    const auto t_post = Clock::now();
+    DeviceBuffer<double> xc64, yc64, x_out, y_out, row_value, col_dual, obj;
+    VJ_TRY(xc64.alloc(n));
+    VJ_TRY(yc64.alloc(m));
+    VJ_TRY(x_out.alloc(n));
+    VJ_TRY(y_out.alloc(m));
+    VJ_TRY(row_value.alloc(m));
+    VJ_TRY(col_dual.alloc(n));
+    VJ_TRY(obj.alloc(1));
+    if (cur_phase == 0) {
+        k_widen<float><<<grid_for(n), kThreads, 0, st>>>(n, p32.xc.get(), xc64.get());
+        k_widen<float><<<grid_for(m), kThreads, 0, st>>>(m, p32.yc.get(), yc64.get());
+    } else {
+        VJ_CUDA(cudaMemcpyAsync(xc64.get(), p64.xc.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        VJ_CUDA(cudaMemcpyAsync(yc64.get(), p64.yc.get(), sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
+    }
+    k_post_vectors<<<grid_for(mx), kThreads, 0, st>>>(m, n, xc64.get(), yc64.get(), p.col_scale.get(), p.row_scale.get(),
+                                                      p.scaled ? 1 : 0, is_max ? 1 : 0, x_out.get(), y_out.get());
+    launch_spmv_t<double, double, double>(a64, p.csr_val_orig.get(), x_out.get(), EpiStore<double>{row_value.get()}, st);
+    launch_spmv_t<double, double, double>(at64, lp.values.get(), y_out.get(), EpiStore<double>{col_dual.get()}, st);
+    k_sub_from<<<grid_for(n), kThreads, 0, st>>>(n, lp.c.get(), col_dual.get());
+    k_dot_offset<<<1, 1024, 0, st>>>(n, lp.c.get(), x_out.get(), h->objective_offset, obj.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(cur_phase == 0 ? 5 : 3);
+    double objective = 0.0;
+    VJ_CUDA(cudaMemcpyAsync(&objective, obj.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hs, S, sizeof(HState), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    const double post_time = seconds_since(t_post);
+
+    dev_timer.stop(st);
+    r->device_time_sec = dev_timer.seconds();
+    const auto t_dl = Clock::now();
+    copy_out_vector(r->col_value, x_out.get(), n, st);
+    copy_out_vector(r->row_value, row_value.get(), m, st);
+    copy_out_vector(r->row_dual, y_out.get(), m, st);
+    copy_out_vector(r->col_dual, col_dual.get(), n, st);
+    VJ_CUDA(cudaStreamSynchronize(st));
+    h->transfers += 4;
+
+    int status = hs->status;
+    if (!hs->stop) status = timed_out ? kStatusTimeLimit : kStatusIterLimit;
+    r->status = status;
+    r->iterations = hs->total;
+    r->objective_value = objective;
+    r->dual_objective = is_max ? -hs->dobj : hs->dobj;
+    r->restart_count = hs->restart_count;
+    r->primal_residual = hs->rel_p;
+    r->dual_residual = hs->rel_d;
+    r->duality_gap = hs->rel_gap;
+    r->spectral_norm_estimate = spectral_norm;
+    r->tau = hs->tau;
+    r->sigma = hs->sigma;
+    r->converged = status == kStatusOptimal ? 1 : 0;
+    r->rel_primal = hs->rel_p;
+    r->rel_dual = hs->rel_d;
+    r->rel_gap = hs->rel_gap;
+    r->rel_kkt = hs->rel_kkt;
+    r->primal_weight = hs->omega;
+    r->fp32_iterations = hs->phase_iters[0];
+    r->fp64_iterations = hs->phase_iters[1];
+    r->setup_time_sec = setup_time;
+    r->iteration_time_sec = iter_time + post_time;
+    r->download_time_sec = seconds_since(t_dl);
+    r->spmv_group_a = a_it.group;
+    r->spmv_group_at = at_it.group;
+    {
+        const bool use32 = mixed && hs->phase_iters[0] >= hs->phase_iters[1];
+        const double vs = use32 ? 4.0 : 8.0;   // value / vector bytes
+        const double nn = static_cast<double>(nnz), dm = m, dn = n;
+        const double t = use32 ? p32.t_primal_ms : p64.t_primal_ms, d = use32 ? p32.t_dual_ms : p64.t_dual_ms;
+        const int64_t ns = use32 ? p32.samples : p64.samples;
+        r->kernel_samples = ns;
+        r->primal_kernel_us = ns ? 1e3 * t / ns : 0.0;
+        r->dual_kernel_us = ns ? 1e3 * d / ns : 0.0;
+        // primal: CSC pointers (int64), indices + values, y gathered once, c/l/u/x/x0 read,
+        // x and x_bar written.  dual: CSR pointers, indices + values, x_bar gathered once,
+        // l/u/y/y0 read, y written.
+        r->primal_kernel_bytes = 8.0 * (dn + 1) + (4.0 + vs) * nn + vs * dm + 7.0 * vs * dn;
+        r->dual_kernel_bytes = 8.0 * (dm + 1) + (4.0 + vs) * nn + vs * dn + 5.0 * vs * dm;
+    }
+    const char* msg = status == kStatusOptimal ? "relative KKT tolerance reached"
+                    : status == kStatusNumerical ? "NaN/Inf in the KKT evaluation"
+                    : status == kStatusTimeLimit ? "time limit reached" : "iteration limit reached";
+    std::snprintf(r->status_message, sizeof(r->status_message), "%s", msg);
+    return VAJRA_OK;
+}
+
 }  // namespace vajra

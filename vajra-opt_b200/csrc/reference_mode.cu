@@ -243,6 +243,8 @@ __global__ void k_reduced_cost(int n, const double* __restrict__ c, double* __re
 vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     const auto t_start = Clock::now();
     cudaStream_t st = h->stream;
+    StreamTimer dev_timer;
+    dev_timer.start(st);
     const vajra_opts& o = h->opts;
     const int m = h->m, n = h->n;
     const int64_t nnz = h->nnz;
@@ -316,6 +318,7 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(v.alloc(n));
     auto enqueue_check = [&](int len) {
         launch_spmv_exact<double, false>(at, p.csc_val.get(), y.get(), EpiStoreRef{v.get(), S}, st);
+        note_launch(2);
         k_ref_check<<<1, 1024, 0, st>>>(m, n, ax.get(), x.get(), y.get(), v.get(), p.c.get(), p.row_lower.get(),
                                         p.row_upper.get(), p.col_lower.get(), p.col_upper.get(), len, check_freq,
                                         tol, gap_tol, safety, S);
@@ -335,18 +338,23 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     const auto t_iter = Clock::now();
     int64_t done_iters = 0;
     int timed_out = 0;
+    int64_t before = 0, graph_kernels = 0;
     while (done_iters < max_iter) {
         const int64_t remaining = max_iter - done_iters;
         const int len = static_cast<int>(remaining < check_freq ? remaining : check_freq);
         if (len == check_freq) {
             if (!exec) {
+                before = launch_count();
                 VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 enqueue_chunk(len);
                 enqueue_check(len);
                 VJ_CUDA(cudaStreamEndCapture(st, &graph));
                 VJ_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+                graph_kernels = launch_count() - before;
+                launch_count() = before;
             }
             VJ_CUDA(cudaGraphLaunch(exec, st));
+            note_launch(graph_kernels);
         } else {
             enqueue_chunk(len);
             enqueue_check(len);
@@ -380,6 +388,8 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     VJ_CUDA(cudaStreamSynchronize(st));
     const double iter_time = seconds_since(t_iter);
 
+    dev_timer.stop(st);
+    r->device_time_sec = dev_timer.seconds();
     const auto t_dl = Clock::now();
     copy_out_vector(r->col_value, x_out.get(), n, st);
     copy_out_vector(r->row_value, row_value.get(), m, st);

@@ -107,6 +107,7 @@ vajra_status build_csr(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
     }
     k_row_ptr_from_sorted<<<grid_stride_blocks(nnz + 1), kThreads, 0, st>>>(nnz, m, keys_out.get(), p.csr_ptr.get());
     VJ_LAUNCH_CHECK();
+    note_launch(3 + (nnz > 0 ? 1 + 4 : 0));   // expand, iota, row_ptr; gather + radix-sort passes
     // Keep the temporaries alive until the work that reads them has run.
     VJ_CUDA(cudaStreamSynchronize(st));
     return VAJRA_OK;
@@ -248,6 +249,7 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
     k_fill<<<grid_stride_blocks(n), kThreads, 0, st>>>(n, p.col_scale.get(), 1.0);
     if (o.negate_c && n > 0) k_negate<<<grid_for(n), kThreads, 0, st>>>(n, p.c.get());
     VJ_LAUNCH_CHECK();
+    note_launch(2 + (o.negate_c && n > 0 ? 1 : 0));
     p.scaled = false;
     if (o.enable && m > 0 && n > 0) {
         DeviceBuffer<double> row_norm, col_norm, r_k, c_k;
@@ -266,6 +268,7 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
             k_scale_matrix<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), lp.row_idx.get(), p.csc_val.get(),
                                                              r_k.get(), c_k.get(), sst, 1);
             VJ_LAUNCH_CHECK();
+            note_launch(6);
         }
         if (o.pock_chambolle) {
             k_col_abs_sum<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), p.csc_val.get(), col_norm.get());
@@ -275,12 +278,14 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
             k_scale_matrix<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), lp.row_idx.get(), p.csc_val.get(),
                                                              r_k.get(), c_k.get(), sst, 0);
             VJ_LAUNCH_CHECK();
+            note_launch(5);
         }
         const int mx = m > n ? m : n;
         k_scale_vectors<<<grid_for(mx), kThreads, 0, st>>>(m, n, p.c.get(), p.row_lower.get(), p.row_upper.get(),
                                                            p.col_lower.get(), p.col_upper.get(),
                                                            p.row_scale.get(), p.col_scale.get());
         VJ_LAUNCH_CHECK();
+        note_launch(1);
         VJ_CUDA(cudaStreamSynchronize(st));   // temporaries above go out of scope
         p.scaled = true;
     }
@@ -290,6 +295,7 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
         k_gather<double><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.perm.get(), p.csc_val.get(), p.csr_val.get());
         k_gather<double><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.perm.get(), lp.values.get(), p.csr_val_orig.get());
         VJ_LAUNCH_CHECK();
+        note_launch(2);
     }
     // CSR views: A over csr_*, A^T over the raw CSC structure.
     p.a.rows = m; p.a.cols = n; p.a.nnz = nnz; p.a.ptr = p.csr_ptr.get(); p.a.idx = p.csr_idx.get();
@@ -304,6 +310,7 @@ vajra_status make_f32_values(Prepared& p, int64_t nnz, cudaStream_t st) {
         k_convert<double, float><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.csc_val.get(), p.csc_val32.get());
         k_convert<double, float><<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.csr_val.get(), p.csr_val32.get());
         VJ_LAUNCH_CHECK();
+        note_launch(2);
     }
     return VAJRA_OK;
 }
@@ -377,9 +384,11 @@ vajra_status spectral_norm_exact(const Prepared& p, int m, int n, int max_iter, 
         k_power_step_exact<<<1, 1, 0, st>>>(n, u.get(), tol, sst);
         k_power_scale<<<grid_for(n), kThreads, 0, st>>>(n, u.get(), v.get(), sst);
         VJ_LAUNCH_CHECK();
+        note_launch(2);
     }
     k_power_final<<<1, 1, 0, st>>>(sst);
     VJ_LAUNCH_CHECK();
+    note_launch(2);   // final + the initial fill
     VJ_CUDA(cudaStreamSynchronize(st));
     return VAJRA_OK;
 }
@@ -429,9 +438,11 @@ vajra_status spectral_norm_fast(const Prepared& p, int m, int n, int max_iter, d
         k_power_step_fast<<<1, kThreads, 0, st>>>(nparts, part.get(), tol, sst);
         k_power_scale<<<grid_for(n), kThreads, 0, st>>>(n, u.get(), v.get(), sst);
         VJ_LAUNCH_CHECK();
+        note_launch(3);
     }
     k_power_final<<<1, 1, 0, st>>>(sst);
     VJ_LAUNCH_CHECK();
+    note_launch(2);
     VJ_CUDA(cudaStreamSynchronize(st));
     return VAJRA_OK;
 }
@@ -464,6 +475,7 @@ static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, cudaStream
     VJ_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int), st));
     if (v.rows > 0) k_collect_long<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, long_len, list.get(), cnt.get());
     VJ_LAUNCH_CHECK();
+    note_launch(v.rows > 0 ? 1 : 0);
     int h = 0;
     VJ_CUDA(cudaMemcpyAsync(&h, cnt.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaStreamSynchronize(st));

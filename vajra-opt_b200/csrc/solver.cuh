@@ -28,9 +28,18 @@ inline double seconds_since(Clock::time_point t0) {
     return std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
-// Copies result vectors / scalars to the caller and records the timing.
-struct HostOut {
-    vajra_result* r;
+// Elapsed time between two points of a stream's timeline (CUDA events).
+struct StreamTimer {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    StreamTimer() { cudaEventCreate(&e0); cudaEventCreate(&e1); }
+    ~StreamTimer() { if (e0) cudaEventDestroy(e0); if (e1) cudaEventDestroy(e1); }
+    void start(cudaStream_t st) { cudaEventRecord(e0, st); }
+    void stop(cudaStream_t st) { cudaEventRecord(e1, st); }
+    double seconds() const {   // call after the stream passed stop()
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) return -1.0;
+        return 1e-3 * ms;
+    }
 };
 
 vajra_status run_reference(vajra_pdhg* h, vajra_result* r);

@@ -86,10 +86,11 @@ k_spmv_seq(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
 }
 
 // ----- fast family --------------------------------------------------------------------
-template <typename V, typename Acc, int G, class Epi>
+// VV: stored value type, VX: dense-vector type, Acc: accumulation type.
+template <typename VV, typename VX, typename Acc, int G, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-           const V* __restrict__ val, const V* __restrict__ x, int64_t long_len,
+           const VV* __restrict__ val, const VX* __restrict__ x, int64_t long_len,
            const int32_t* __restrict__ long_rows, int vec_blocks, Epi epi) {
     if (!epi.active()) return;
     if (static_cast<int>(blockIdx.x) >= vec_blocks) {
@@ -139,30 +140,38 @@ struct CsrView {
     int n_long = 0;
 };
 
-template <typename V, typename Acc, int G, class Epi>
-inline void launch_vec_g(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
+template <typename VV, typename VX, typename Acc, int G, class Epi>
+inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     const int vec_blocks = static_cast<int>(grid_for(static_cast<int64_t>(a.rows) * G));
-    k_spmv_vec<V, Acc, G, Epi><<<vec_blocks + a.n_long, kThreads, 0, st>>>(
+    k_spmv_vec<VV, VX, Acc, G, Epi><<<vec_blocks + a.n_long, kThreads, 0, st>>>(
         a.rows, a.ptr, a.idx, val, x, a.long_len, a.long_rows, vec_blocks, epi);
+    note_launch();
+}
+
+// Lane-group sizes other than 1..16 dispatch to 32.
+template <typename VV, typename VX, typename Acc, class Epi>
+inline void launch_spmv_t(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
+    if (a.rows <= 0) return;
+    switch (a.group) {
+        case 1: launch_vec_g<VV, VX, Acc, 1>(a, val, x, epi, st); break;
+        case 2: launch_vec_g<VV, VX, Acc, 2>(a, val, x, epi, st); break;
+        case 4: launch_vec_g<VV, VX, Acc, 4>(a, val, x, epi, st); break;
+        case 8: launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st); break;
+        case 16: launch_vec_g<VV, VX, Acc, 16>(a, val, x, epi, st); break;
+        default: launch_vec_g<VV, VX, Acc, 32>(a, val, x, epi, st); break;
+    }
 }
 
 template <typename V, typename Acc, class Epi>
 inline void launch_spmv(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
-    if (a.rows <= 0) return;
-    switch (a.group) {
-        case 1: launch_vec_g<V, Acc, 1>(a, val, x, epi, st); break;
-        case 2: launch_vec_g<V, Acc, 2>(a, val, x, epi, st); break;
-        case 4: launch_vec_g<V, Acc, 4>(a, val, x, epi, st); break;
-        case 8: launch_vec_g<V, Acc, 8>(a, val, x, epi, st); break;
-        case 16: launch_vec_g<V, Acc, 16>(a, val, x, epi, st); break;
-        default: launch_vec_g<V, Acc, 32>(a, val, x, epi, st); break;
-    }
+    launch_spmv_t<V, V, Acc>(a, val, x, epi, st);
 }
 
 template <typename V, bool ZERO_DROP, class Epi>
 inline void launch_spmv_exact(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
     if (a.rows <= 0) return;
     k_spmv_seq<V, ZERO_DROP, Epi><<<grid_for(a.rows), kThreads, 0, st>>>(a.rows, a.ptr, a.idx, val, x, epi);
+    note_launch();
 }
 
 }  // namespace vajra

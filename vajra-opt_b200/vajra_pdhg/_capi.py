@@ -53,7 +53,10 @@ class VajraResult(C.Structure):
                 ("iteration_time_sec", C.c_double), ("download_time_sec", C.c_double),
                 ("total_time_sec", C.c_double), ("host_device_transfers", C.c_int64),
                 ("spmv_group_a", C.c_int32), ("spmv_group_at", C.c_int32),
-                ("status_message", C.c_char * 256)]
+                ("primal_kernel_us", C.c_double), ("dual_kernel_us", C.c_double),
+                ("primal_kernel_bytes", C.c_double), ("dual_kernel_bytes", C.c_double),
+                ("kernel_samples", C.c_int64), ("kernel_launches", C.c_int64),
+                ("device_time_sec", C.c_double), ("status_message", C.c_char * 256)]
 
 
 class VajraDeviceInfo(C.Structure):
