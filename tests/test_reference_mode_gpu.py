@@ -22,7 +22,7 @@ def run_both(lp, iters, cf=100, tol=1e-6, gap_tol=1e-6, scale=True, compare_col_
     for k in keys:
         np.testing.assert_array_equal(g[k], o[k], err_msg=k)
     for k in SCALARS:
-        assert g[k] == o[k], (k, g[k], o[k])
+        assert g[k] == o[k] or (np.isnan(g[k]) and np.isnan(o[k])), (k, g[k], o[k])
     return g, o
 
 
