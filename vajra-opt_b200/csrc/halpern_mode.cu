@@ -345,12 +345,17 @@ k_norms(int m, int n, const double* __restrict__ rl_o, const double* __restrict_
     if (threadIdx.x == 0) for (int q = 0; q < 4; ++q) out[q] = sqrt(v[q]);
 }
 
+// Unscale and map to the verifier's conventions.  The row dual is the minimisation-form
+// multiplier for both senses, which is what verifier::verify_solution and
+// Solution::recompute_quality check (src/engine/verifier.cpp:172-262, model.cpp:286-364).
+// (The reference PDHG returns +y for maximisation, pdhg.cpp:409-411, which its own verifier
+// rejects; VAJRA_ALGO_REFERENCE keeps that for parity.)
 __global__ void k_post_vectors(int m, int n, const double* __restrict__ xc, const double* __restrict__ yc,
-                               const double* __restrict__ cs, const double* __restrict__ rs, int scaled, int is_max,
+                               const double* __restrict__ cs, const double* __restrict__ rs, int scaled,
                                double* __restrict__ x_out, double* __restrict__ y_out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x_out[i] = scaled ? xc[i] * cs[i] : xc[i];
-    if (i < m) { const double v = scaled ? yc[i] * rs[i] : yc[i]; y_out[i] = is_max ? v : -v; }
+    if (i < m) { const double v = scaled ? yc[i] * rs[i] : yc[i]; y_out[i] = -v; }
 }
 
 template <typename T>
@@ -368,9 +373,11 @@ k_dot_offset(int n, const double* __restrict__ a, const double* __restrict__ b, 
     if (threadIdx.x == 0) *out = offset + v[0];
 }
 
-__global__ void k_sub_from(int n, const double* __restrict__ c, double* __restrict__ d) {
+// Reduced costs as recompute_quality defines them (model.cpp:303-307): d = c - A^T y for
+// minimisation, c + A^T y for maximisation (the sign-flipped min-form reduced cost).
+__global__ void k_reduced_costs(int n, const double* __restrict__ c, int is_max, double* __restrict__ d) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) d[j] = c[j] - d[j];
+    if (j < n) d[j] = is_max ? c[j] + d[j] : c[j] - d[j];
 }
 
 // One precision's iterate set, kernels and captured chunk graph.
@@ -450,9 +457,10 @@ void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const 
 template <typename T>
 void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrView& a64, const CsrView& at64,
                    const Prepared& p, const DeviceLp& lp, CheckBuffers& cb, HState* S, double gamma, int len,
-                   ControlParams cp, cudaStream_t st) {
+                   ControlParams cp, bool capturing, cudaStream_t st) {
+    // Event-record nodes (cudaEventRecordExternal) exist only inside a stream capture.
     for (int kk = 0; kk < len; ++kk)
-        enqueue_iteration(ph, a, at, S, gamma, kk, kk == len - 1 ? 1 : 0, kk == 0 && len > 1, st);
+        enqueue_iteration(ph, a, at, S, gamma, kk, kk == len - 1 ? 1 : 0, kk == 0 && capturing, st);
     cp.len = len;
     cp.phase = ph.phase;
     enqueue_check(ph, a64, at64, p, lp, cb, S, cp, st);
@@ -557,7 +565,12 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // Launch shapes: FP64 views for the checks, autotuned views for the iteration precision.
     CsrView a64 = p.a, at64 = p.at;
     CsrView a_it = p.a, at_it = p.at;
-    if (o.autotune) {
+    if (o.autotune && h->tuned_group_a > 0) {
+        a_it.group = h->tuned_group_a;
+        at_it.group = h->tuned_group_at;
+        a64.group = a_it.group;
+        at64.group = at_it.group;
+    } else if (o.autotune) {
         if (mixed) {
             VJ_TRY(autotune<float>(a_it, p.csr_val32.get(), p32.xb.get(), p32.yc.get(), st));
             VJ_TRY(autotune<float>(at_it, p.csc_val32.get(), p32.y.get(), p32.xc.get(), st));
@@ -567,6 +580,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         }
         a64.group = a_it.group;
         at64.group = at_it.group;
+        h->tuned_group_a = a_it.group;
+        h->tuned_group_at = at_it.group;
     }
 
     const int mx = m > n ? m : n;
@@ -629,7 +644,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 if (!ph.exec) {
                     const int64_t before = launch_count();
                     VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                    enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, st);
+                    enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, true, st);
                     VJ_CUDA(cudaStreamEndCapture(st, &ph.graph));
                     VJ_CUDA(cudaGraphInstantiate(&ph.exec, ph.graph, 0));
                     ph.graph_kernels = launch_count() - before;
@@ -638,7 +653,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 VJ_CUDA(cudaGraphLaunch(ph.exec, st));
                 note_launch(ph.graph_kernels);
             } else {
-                enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, st);
+                enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, false, st);
                 VJ_LAUNCH_CHECK();
             }
             return VAJRA_OK;
@@ -695,10 +710,10 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         VJ_CUDA(cudaMemcpyAsync(yc64.get(), p64.yc.get(), sizeof(double) * m, cudaMemcpyDeviceToDevice, st));
     }
     k_post_vectors<<<grid_for(mx), kThreads, 0, st>>>(m, n, xc64.get(), yc64.get(), p.col_scale.get(), p.row_scale.get(),
-                                                      p.scaled ? 1 : 0, is_max ? 1 : 0, x_out.get(), y_out.get());
+                                                      p.scaled ? 1 : 0, x_out.get(), y_out.get());
     launch_spmv_t<double, double, double>(a64, p.csr_val_orig.get(), x_out.get(), EpiStore<double>{row_value.get()}, st);
     launch_spmv_t<double, double, double>(at64, lp.values.get(), y_out.get(), EpiStore<double>{col_dual.get()}, st);
-    k_sub_from<<<grid_for(n), kThreads, 0, st>>>(n, lp.c.get(), col_dual.get());
+    k_reduced_costs<<<grid_for(n), kThreads, 0, st>>>(n, lp.c.get(), is_max ? 1 : 0, col_dual.get());
     k_dot_offset<<<1, 1024, 0, st>>>(n, lp.c.get(), x_out.get(), h->objective_offset, obj.get());
     VJ_LAUNCH_CHECK();
     note_launch(cur_phase == 0 ? 5 : 3);

@@ -19,6 +19,10 @@ struct vajra_pdhg {
     std::vector<double> h_c, h_cl, h_cu, h_rl, h_ru;   // only kept for m == 0 / nnz == 0
     double upload_time_sec = 0.0;
     int64_t transfers = 0;
+    // SpMV lane groups chosen by the first autotuned run of this handle; later runs reuse
+    // them, so repeated runs of one handle sum in the same order and repeat bit for bit.
+    int tuned_group_a = 0;
+    int tuned_group_at = 0;
 };
 
 namespace vajra {

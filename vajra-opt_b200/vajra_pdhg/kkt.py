@@ -11,8 +11,9 @@ KKT figure.  Definitions (minimisation form; a maximisation LP is negated first)
                src/solvers/pdhg/pdhg.cpp:279-313 evaluated at (y, lambda)
   rel_kkt    = max of the three
 
-||b|| counts every finite row bound, an equality row once.  y is the row dual in the
-verifier's sign convention (<= row: y <= 0, >= row: y >= 0), as vajra_result.row_dual.
+||b|| counts every finite row bound, an equality row once.  y is the row dual of the
+minimisation form in the verifier's sign convention (<= row: y <= 0, >= row: y >= 0) for both
+objective senses, as VAJRA_ALGO_HALPERN returns it in vajra_result.row_dual.
 """
 from __future__ import annotations
 
@@ -25,7 +26,7 @@ def relative_kkt(lp, x, row_dual) -> dict:
     A = lp.to_scipy_csc()
     is_max = int(getattr(lp, "sense", 0)) != 0
     c = -np.asarray(lp.c, float) if is_max else np.asarray(lp.c, float)
-    y = -np.asarray(row_dual, float) if is_max else np.asarray(row_dual, float)
+    y = np.asarray(row_dual, float)
     off = float(getattr(lp, "objective_offset", 0.0))
     off = -off if is_max else off
     rl, ru = np.asarray(lp.row_lower, float), np.asarray(lp.row_upper, float)
