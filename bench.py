@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-iters", type=int, default=0,
+                    help="profiling aid: one solve capped at this many iterations, then exit (for ncu)")
+    ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed")
     return ap.parse_args()
 
 
@@ -223,6 +226,15 @@ def main():
 
     torch.cuda.set_device(local)
     lp = W.random_large(args.rows, args.cols, seed=args.seed + rank)
+    if args.profile_iters > 0:
+        prec = V.PREC_MIXED if args.profile_precision == "mixed" else V.PREC_FP64
+        r = V.solve(lp, precision=prec, iteration_limit=args.profile_iters, device=local,
+                    mixed_switch_tolerance=0.0, mixed_stall_checks=0)
+        print(json.dumps({"profile_iters": r["iterations"], "status": r["status_name"], "rel_kkt": r["rel_kkt"],
+                          "groups": [r["spmv_group_a"], r["spmv_group_at"]],
+                          "primal_us": r["primal_kernel_us"], "dual_us": r["dual_kernel_us"],
+                          "primal_bytes": r["primal_kernel_bytes"], "dual_bytes": r["dual_kernel_bytes"]}))
+        return 0
     plp = pinned_copy(lp)
 
     def barrier():

@@ -109,8 +109,15 @@ typedef struct vajra_opts {
                                       relative KKT (or when FP32 stalls)                 */
     int32_t device;             /* CUDA device ordinal                                   */
     int32_t autotune;           /* 1 = time SpMV variants at set-up and keep the fastest */
-    int32_t verbose;
-    int32_t reserved[7];
+    int32_t verbose;            /* 1 = one line per check on stderr                      */
+    int32_t mixed_stall_checks; /* MIXED: hand over when 10 checks gained < 5 % (0 = never) */
+    /* HALPERN restart and step parameters */
+    double restart_sufficient;  /* restart when weighted KKT <= this x its restart value (0.2) */
+    double restart_necessary;   /* ... or <= this x and rising (0.8)                     */
+    double restart_artificial;  /* ... or inner iterations >= this x total (0.36)        */
+    double primal_weight_smoothing; /* theta of omega <- exp(theta log(dy/dx) + (1-theta) log omega) (0.5) */
+    double step_safety;         /* eta = step_safety / ||A||_2 (0.99)                    */
+    int32_t reserved[6];
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and
@@ -148,8 +155,10 @@ typedef struct vajra_result {
     double download_time_sec;
     double total_time_sec;
     int64_t host_device_transfers;
-    int32_t spmv_group_a;       /* lanes per row chosen for A x      (0 = sequential)     */
-    int32_t spmv_group_at;      /* lanes per row chosen for A^T y                          */
+    int32_t spmv_group_a;       /* SpMV shape chosen for A x: 1..32 lanes per row, 0 the
+                                   shared-memory row-block kernel, -1 the exact in-order
+                                   kernel of VAJRA_ALGO_REFERENCE                            */
+    int32_t spmv_group_at;      /* same for A^T y                                           */
     /* Live kernel timing (HALPERN): CUDA-event durations of the fused iteration kernels,
      * sampled on the solve's stream once per check interval, for the precision that ran
      * most iterations, with the algorithmic bytes one launch must move. */

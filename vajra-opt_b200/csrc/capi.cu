@@ -183,6 +183,12 @@ void vajra_default_opts(vajra_opts* o) {
     o->device = 0;
     o->autotune = 1;
     o->verbose = 0;
+    o->mixed_stall_checks = 10;
+    o->restart_sufficient = 0.2;
+    o->restart_necessary = 0.8;
+    o->restart_artificial = 0.36;
+    o->primal_weight_smoothing = 0.5;
+    o->step_safety = 0.99;
 }
 
 vajra_status vajra_probe_device(int32_t device, vajra_device_info* info) {

@@ -61,10 +61,13 @@ public:
         if (this != &o) { reset(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
         return *this;
     }
+    // Every allocation carries kPad spare elements, so 128-bit vector loads of the last
+    // aligned group of four never leave the allocation (their extra lanes are masked).
+    static constexpr size_t kPad = 16;
     vajra_status alloc(size_t n) {
         reset();
         if (n == 0) n = 1;   // keep a valid pointer for empty extents
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p_), n * sizeof(T));
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p_), (n + kPad) * sizeof(T));
         if (e != cudaSuccess) { p_ = nullptr; return cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
         n_ = n;
         return VAJRA_OK;

@@ -199,6 +199,7 @@ struct ControlParams {
     int len;          // iterations in the chunk just finished
     int phase;
     int mixed;        // 1 when an FP32 phase hands over to FP64
+    int stall_checks; // FP32 stall window in checks (0 = no stall test; at most kHist - 1)
 };
 
 __global__ void __launch_bounds__(1024)
@@ -246,9 +247,10 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
     const double wk = sqrt(omega * rp_s2 + rd_s2 / omega + rel_gap * rel_gap);
     if (cp.mixed && cp.phase == 0) {
         const int hn = st->hist_n;
+        const int w = cp.stall_checks;
         bool stalled = false;
-        if (hn >= 10) {
-            const double old = st->hist[(hn - 10) % kHist];
+        if (w > 0 && hn >= w) {
+            const double old = st->hist[(hn - w) % kHist];
             stalled = rel > 0.95 * old;
         }
         st->hist[hn % kHist] = rel;
@@ -475,7 +477,7 @@ vajra_status autotune(CsrView& v, const T* val, const T* xin, T* out, cudaStream
     VJ_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     int best_g = v.group;
-    for (int g : {1, 2, 4, 8, 16, 32}) {
+    for (int g : {0, 1, 2, 4, 8, 16, 32}) {   // 0: row-block kernel, else lanes per row
         CsrView t = v;
         t.group = g;
         launch_spmv_t<T, T, T>(t, val, xin, EpiStore<T>{out}, st);     // warm
@@ -597,7 +599,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     note_launch(1);
 
     HState init{};
-    const double eta = 0.99 / spectral_norm;
+    const double eta = (o.step_safety > 0.0 && o.step_safety < 1.0 ? o.step_safety : 0.99) / spectral_norm;
     init.omega = (hn[2] > 1e-10 && hn[3] > 1e-10) ? hn[3] / hn[2] : 1.0;
     init.eta = eta;
     init.tau = eta / init.omega;
@@ -623,11 +625,12 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     ControlParams cp{};
     cp.tol = o.tolerance;
     cp.switch_tol = o.mixed_switch_tolerance;
-    cp.beta_sufficient = 0.2;
-    cp.beta_necessary = 0.8;
-    cp.beta_artificial = 0.36;
-    cp.pw_smoothing = 0.5;
+    cp.beta_sufficient = o.restart_sufficient;
+    cp.beta_necessary = o.restart_necessary;
+    cp.beta_artificial = o.restart_artificial;
+    cp.pw_smoothing = o.primal_weight_smoothing;
     cp.mixed = mixed ? 1 : 0;
+    cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
     const double gamma = o.reflection;
     const int K = o.check_frequency > 0 ? o.check_frequency : 64;
     const int64_t max_iter = o.iteration_limit;
@@ -688,6 +691,10 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             note_launch(1);
             cur_phase = hs->phase;
         }
+        if (o.verbose)
+            std::fprintf(stderr, "[vajra] it %lld phase %d rel_kkt %.3e (p %.2e d %.2e gap %.2e) omega %.4g restarts %d\n",
+                         hs->total, hs->phase, hs->rel_kkt, hs->rel_p, hs->rel_d, hs->rel_gap, hs->omega,
+                         hs->restart_count);
         if (seconds_since(t_start) > o.time_limit) { timed_out = 1; break; }
     }
     const double iter_time = seconds_since(t_iter);

@@ -40,6 +40,8 @@ struct Prepared {
     DeviceBuffer<double> row_scale, col_scale;
     // per-row / per-column lists of long rows for the fast SpMV
     DeviceBuffer<int32_t> long_rows_a, long_rows_at;
+    // row-block partitions (block boundaries) and their rows longer than kTile
+    DeviceBuffer<int32_t> rb_blocks_a, rb_blocks_at, rb_long_a, rb_long_at;
     bool scaled = false;
     CsrView a, at;                            // A (rows = m) and A^T (rows = n)
 };

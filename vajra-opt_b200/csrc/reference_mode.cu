@@ -414,8 +414,8 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     r->setup_time_sec = setup_time;
     r->iteration_time_sec = iter_time;
     r->download_time_sec = seconds_since(t_dl);
-    r->spmv_group_a = 0;
-    r->spmv_group_at = 0;
+    r->spmv_group_a = -1;
+    r->spmv_group_at = -1;
     const char* msg = "";
     switch (hs->status) {
         case kStatusOptimal: msg = "PDHG converged to optimal primal and dual tolerance"; break;

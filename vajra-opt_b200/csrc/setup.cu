@@ -463,12 +463,24 @@ static int default_group(double mean_len) {
     return g;
 }
 
-static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, cudaStream_t st) {
-    const double mean = v.rows > 0 ? static_cast<double>(v.nnz) / v.rows : 0.0;
-    v.group = default_group(mean);
-    int64_t long_len = static_cast<int64_t>(8.0 * mean);
-    if (long_len < 256) long_len = 256;
-    v.long_len = long_len;
+// block_rows[b] = first row whose first entry is at or after b * tile (binary search over
+// ptr[0..rows]); block_rows[nb] = rows.
+__global__ void k_rowblock_partition(int rows, const int64_t* __restrict__ ptr, int64_t tile, int nb,
+                                     int32_t* __restrict__ block_rows) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nb) return;
+    if (b == nb) { block_rows[b] = rows; return; }
+    const int64_t target = static_cast<int64_t>(b) * tile;
+    int lo = 0, hi = rows;
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (ptr[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    block_rows[b] = lo;
+}
+
+static vajra_status collect_long(const CsrView& v, int64_t long_len, DeviceBuffer<int32_t>& list, int* count,
+                                 cudaStream_t st) {
     VJ_TRY(list.alloc(static_cast<size_t>(v.rows > 0 ? v.rows : 1)));
     DeviceBuffer<int> cnt;
     VJ_TRY(cnt.alloc(1));
@@ -479,15 +491,39 @@ static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, cudaStream
     int h = 0;
     VJ_CUDA(cudaMemcpyAsync(&h, cnt.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaStreamSynchronize(st));
-    v.n_long = h;
+    *count = h;
+    return VAJRA_OK;
+}
+
+static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, DeviceBuffer<int32_t>& blocks,
+                             DeviceBuffer<int32_t>& rb_list, cudaStream_t st) {
+    const double mean = v.rows > 0 ? static_cast<double>(v.nnz) / v.rows : 0.0;
+    v.group = default_group(mean);
+    int64_t long_len = static_cast<int64_t>(8.0 * mean);
+    if (long_len < 256) long_len = 256;
+    v.long_len = long_len;
+    VJ_TRY(collect_long(v, long_len, list, &v.n_long, st));
     v.long_rows = list.get();
+    // row-block partition
+    int64_t nb64 = (v.nnz + kTile - 1) / kTile;
+    if (nb64 < 1) nb64 = 1;
+    if (nb64 > (1LL << 30)) { set_error("matrix too large for the row-block partition"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    v.nb = static_cast<int>(nb64);
+    VJ_TRY(blocks.alloc(static_cast<size_t>(v.nb) + 1));
+    k_rowblock_partition<<<grid_for(static_cast<int64_t>(v.nb) + 1), kThreads, 0, st>>>(v.rows, v.ptr, kTile, v.nb,
+                                                                                        blocks.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
+    v.block_rows = blocks.get();
+    VJ_TRY(collect_long(v, kTile, rb_list, &v.rb_n_long, st));
+    v.rb_long_rows = rb_list.get();
     return VAJRA_OK;
 }
 
 vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
     (void)lp;
-    VJ_TRY(plan_one(p.a, p.long_rows_a, st));
-    VJ_TRY(plan_one(p.at, p.long_rows_at, st));
+    VJ_TRY(plan_one(p.a, p.long_rows_a, p.rb_blocks_a, p.rb_long_a, st));
+    VJ_TRY(plan_one(p.at, p.long_rows_at, p.rb_blocks_at, p.rb_long_at, st));
     return VAJRA_OK;
 }
 

@@ -126,6 +126,102 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
     if (valid && lane == 0) epi(row, acc);
 }
 
+// ----- row-block family (shared-memory staging) ----------------------------------------
+// The rows are cut into blocks of consecutive rows: block b holds the rows whose first entry
+// lies in [b*kTile, (b+1)*kTile) (a binary search per block at set-up).  A CTA streams its
+// block's indices and values with 128-bit vector loads (aligned groups of four; the partial
+// groups at both ends are masked), issues every gather of the dense vector independently,
+// and stages the products in shared memory.  Then each short row is summed by one thread in
+// storage order and rows longer than kMediumRow by one warp (fixed butterfly), and the
+// epilogue runs on consecutive rows, so its vector loads and stores coalesce.  A row longer
+// than kTile is necessarily the last row starting in its block; it is taken by one of the
+// trailing CTAs of the same launch.  A block's staged entries never exceed 2 kTile - 1.
+constexpr int kTile = 2048;
+constexpr int kMediumRow = 48;
+constexpr int kMaxMediumRows = (2 * kTile) / kMediumRow + 1;
+
+__device__ __forceinline__ void load4(const int32_t* p, int (&v)[4]) {
+    const int4 t = __ldcs(reinterpret_cast<const int4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void load4(const float* p, float (&v)[4]) {
+    const float4 t = __ldcs(reinterpret_cast<const float4*>(p));
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
+    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2*>(p + 2));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+template <typename VV, typename VX, typename Acc, class Epi>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const VV* __restrict__ val,
+                const VX* __restrict__ x, const int32_t* __restrict__ block_rows, int nb,
+                const int32_t* __restrict__ long_rows, Epi epi) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Acc* prod = reinterpret_cast<Acc*>(smem_raw);
+    __shared__ int med_rows[kMaxMediumRows];
+    __shared__ int n_med;
+    __shared__ Acc red[32];
+    if (!epi.active()) return;
+    if (static_cast<int>(blockIdx.x) >= nb) {
+        const int row = long_rows[blockIdx.x - nb];
+        const int64_t s = ptr[row], e = ptr[row + 1];
+        Acc acc = Acc(0);
+        for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+        Acc v[1] = {acc};
+        block_reduce<OpSum, Acc, 1>(v, red);
+        if (threadIdx.x == 0) epi(row, v[0]);
+        return;
+    }
+    const int r0 = block_rows[blockIdx.x], r1 = block_rows[blockIdx.x + 1];
+    if (r0 >= r1) return;
+    int r_end = r1;
+    if (ptr[r1] - ptr[r1 - 1] > kTile) r_end = r1 - 1;
+    const int64_t e0 = ptr[r0], e1 = ptr[r_end];
+    for (int64_t q = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x); q < e1; q += 4 * blockDim.x) {
+        int ii[4];
+        VV vv[4];
+        load4(idx + q, ii);
+        load4(val + q, vv);
+        Acc pr[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int64_t k = q + t;
+            pr[t] = (k >= e0 && k < e1) ? static_cast<Acc>(vv[t]) * static_cast<Acc>(ld_cached(x + ii[t])) : Acc(0);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int64_t k = q + t;
+            if (k >= e0 && k < e1) prod[k - e0] = pr[t];
+        }
+    }
+    if (threadIdx.x == 0) n_med = 0;
+    __syncthreads();
+    for (int r = r0 + threadIdx.x; r < r_end; r += blockDim.x) {
+        const int s = static_cast<int>(ptr[r] - e0), e = static_cast<int>(ptr[r + 1] - e0);
+        if (e - s > kMediumRow) {
+            med_rows[atomicAdd(&n_med, 1)] = r;
+            continue;
+        }
+        Acc acc = Acc(0);
+        for (int k = s; k < e; ++k) acc += prod[k];
+        epi(r, acc);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int w = warp; w < n_med; w += blockDim.x >> 5) {
+        const int r = med_rows[w];
+        const int s = static_cast<int>(ptr[r] - e0), e = static_cast<int>(ptr[r + 1] - e0);
+        Acc acc = Acc(0);
+        for (int k = s + lane; k < e; k += 32) acc += prod[k];
+        acc = warp_reduce<OpSum>(acc);
+        if (lane == 0) epi(r, acc);
+    }
+}
+
 // Host-side description of one SpMV operand (a CSR, possibly the stored transpose) and the
 // launch shape the autotuner chose for it.
 struct CsrView {
@@ -134,11 +230,23 @@ struct CsrView {
     int64_t nnz = 0;
     const int64_t* ptr = nullptr;
     const int32_t* idx = nullptr;
-    int group = 8;                      // lanes per row (1,2,4,...,32)
-    int64_t long_len = 1 << 30;         // rows longer than this go one CTA per row
+    int group = 8;                      // lanes per row (1,2,4,...,32); 0 = row-block kernel
+    int64_t long_len = 1 << 30;         // grouped-lane kernel: rows longer than this go one CTA per row
     const int32_t* long_rows = nullptr; // device list of those rows
     int n_long = 0;
+    const int32_t* block_rows = nullptr;  // row-block kernel: nb + 1 block boundaries
+    int nb = 0;
+    const int32_t* rb_long_rows = nullptr;  // rows longer than kTile
+    int rb_n_long = 0;
 };
+
+template <typename VV, typename VX, typename Acc, class Epi>
+inline void launch_rowblock(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
+    const size_t smem = sizeof(Acc) * 2 * kTile;
+    k_spmv_rowblock<VV, VX, Acc, Epi><<<a.nb + a.rb_n_long, kThreads, smem, st>>>(
+        a.ptr, a.idx, val, x, a.block_rows, a.nb, a.rb_long_rows, epi);
+    note_launch();
+}
 
 template <typename VV, typename VX, typename Acc, int G, class Epi>
 inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
@@ -148,11 +256,15 @@ inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, 
     note_launch();
 }
 
-// Lane-group sizes other than 1..16 dispatch to 32.
+// group 0 selects the row-block kernel; other lane-group sizes than 1..16 dispatch to 32.
 template <typename VV, typename VX, typename Acc, class Epi>
 inline void launch_spmv_t(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     if (a.rows <= 0) return;
     switch (a.group) {
+        case 0:
+            if (a.block_rows) { launch_rowblock<VV, VX, Acc>(a, val, x, epi, st); break; }
+            launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st);
+            break;
         case 1: launch_vec_g<VV, VX, Acc, 1>(a, val, x, epi, st); break;
         case 2: launch_vec_g<VV, VX, Acc, 2>(a, val, x, epi, st); break;
         case 4: launch_vec_g<VV, VX, Acc, 4>(a, val, x, epi, st); break;

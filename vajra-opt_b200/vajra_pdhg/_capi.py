@@ -36,7 +36,10 @@ class VajraOpts(C.Structure):
                 ("enable_scaling", C.c_int32), ("pock_chambolle", C.c_int32),
                 ("ruiz_iterations", C.c_int32), ("reflection", C.c_double),
                 ("mixed_switch_tolerance", C.c_double), ("device", C.c_int32),
-                ("autotune", C.c_int32), ("verbose", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("autotune", C.c_int32), ("verbose", C.c_int32), ("mixed_stall_checks", C.c_int32),
+                ("restart_sufficient", C.c_double), ("restart_necessary", C.c_double),
+                ("restart_artificial", C.c_double), ("primal_weight_smoothing", C.c_double),
+                ("step_safety", C.c_double), ("reserved", C.c_int32 * 6)]
 
 
 class VajraResult(C.Structure):
