@@ -222,6 +222,13 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
  * (pdhg_cuda.cu:187-227 upload once): create uploads the LP to the device; run does the
  * device set-up and the solve from the resident copy; destroy frees it. */
 vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra_pdhg** handle);
+/* Batched form: `count` independent LPs solved together (VAJRA_ALGO_HALPERN, FP64), packed
+ * block-diagonally into one device problem with per-instance step sizes, primal weights,
+ * restarts and termination.  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
+ * the reference's benchmark Suite 2 issues them (apps/benchmark_runner.cpp:936-944).
+ * results[i] receives instance i; every result's device_time_sec is the whole batch's. */
+vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const vajra_opts* opts,
+                                    vajra_result* results);
 vajra_status vajra_pdhg_run(vajra_pdhg* handle, vajra_result* result);
 vajra_status vajra_pdhg_destroy(vajra_pdhg* handle);
 

@@ -92,3 +92,14 @@ def test_no_device_means_no_solve():
     assert info["available"] == 0 and "None" in info["device_name"]
     with pytest.raises(RuntimeError):
         V.solve(lp)
+
+
+@pytest.mark.skipif(cuda_device_present(), reason="checks the no-device path")
+def test_batch_without_device_and_invalid_instances():
+    lps = [W.random_planted(10, 20, 2, seed=s) for s in range(3)]
+    with pytest.raises(RuntimeError, match="no CUDA device|vajra_pdhg_solve_batch failed"):
+        V.solve_batch(lps)
+    bad = W.LP(**{**lps[1].__dict__})
+    bad.col_lower = lps[1].col_lower.copy(); bad.col_lower[0] = 20.0
+    with pytest.raises(RuntimeError):
+        V.solve_batch([lps[0], bad])

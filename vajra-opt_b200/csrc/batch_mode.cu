@@ -1,0 +1,669 @@
+// Batched restarted Halpern PDHG: many independent LPs of uneven sizes packed
+// block-diagonally into one device problem (FP64 iterates, the plain form).
+//
+// The packed matrix diag(A_1, ..., A_B) is one CSC / CSR, so each iteration is still two
+// fused SpMV launches over all instances.  Every instance keeps its own step sizes, primal
+// weight, Halpern counter, restart state and termination flag in device arrays (struct of
+// arrays below); the epilogues look up a row's / column's instance.  Row blocks and rows that
+// belong only to finished instances are skipped before any load, so the work shrinks as
+// instances converge.  Every check interval one CTA per instance reduces that instance's KKT
+// terms, one thread per instance runs the restart / primal-weight / termination logic
+// (same rules as the single-LP solver), and the host reads one counter of active
+// instances.  A chunk of iterations plus its check is one CUDA graph launch; no kernel waits
+// on another kernel, so nothing in this path can spin.
+//
+// Differences from solving the instances one by one: the Ruiz stopping test is evaluated
+// over the packed matrix (all instances take the same number of passes), and the power
+// iteration runs a fixed 60 rounds for every instance.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace vajra {
+namespace {
+
+constexpr int kBQ = 10;   // per-instance check sums
+
+struct BatchArrays {      // device struct of arrays, B entries each
+    double* omega; double* eta; double* tau; double* sigma;
+    double* kkt_start; double* kkt_prev;
+    double* rel_p; double* rel_d; double* rel_gap; double* rel_kkt; double* pobj; double* dobj;
+    double* bnorm; double* cnorm; double* offset_min; double* lambda;
+    long long* k_base; long long* total;
+    int* done; int* status; int* restart_count; int* restart_flag;
+};
+
+struct BatchCounters {
+    int active;
+    int pad;
+};
+
+__device__ __forceinline__ bool any_active(const int* done, const int* inst, int r0, int r1) {
+    const int a = inst[r0], b = inst[r1 - 1];
+    for (int i = a; i <= b; ++i)
+        if (!done[i]) return true;
+    return false;
+}
+
+struct EpiBPrimal {
+    const double* c; const double* cl; const double* cu; const double* x0;
+    double* x; double* xb; double* xc;
+    const int* col_inst;
+    BatchArrays S;
+    double gamma;
+    int kk, write_cand;
+    __device__ bool active() const { return true; }
+    __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, col_inst, r0, r1); }
+    __device__ void operator()(int j, double v) const {
+        const int i = col_inst[j];
+        if (S.done[i]) return;
+        const double k = static_cast<double>(S.k_base[i] + kk);
+        const double w1 = (k + 1.0) / (k + 2.0), w0 = 1.0 / (k + 2.0);
+        const double xo = x[j];
+        double xp = xo - S.tau[i] * (c[j] + v);
+        xp = xp < cl[j] ? cl[j] : (xp > cu[j] ? cu[j] : xp);
+        xb[j] = xp + xp - xo;
+        x[j] = w1 * ((1.0 + gamma) * xp - gamma * xo) + w0 * x0[j];
+        if (write_cand) xc[j] = xp;
+    }
+};
+
+struct EpiBDual {
+    const double* rl; const double* ru; const double* y0;
+    double* y; double* yc;
+    const int* row_inst;
+    BatchArrays S;
+    double gamma;
+    int kk, write_cand;
+    __device__ bool active() const { return true; }
+    __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, row_inst, r0, r1); }
+    __device__ void operator()(int r, double w) const {
+        const int i = row_inst[r];
+        if (S.done[i]) return;
+        const double k = static_cast<double>(S.k_base[i] + kk);
+        const double w1 = (k + 1.0) / (k + 2.0), w0 = 1.0 / (k + 2.0);
+        const double sg = S.sigma[i];
+        const double yo = y[r];
+        const double yh = yo + sg * w;
+        double q = yh / sg;
+        q = q < rl[r] ? rl[r] : (q > ru[r] ? ru[r] : q);
+        const double yp = yh - sg * q;
+        y[r] = w1 * ((1.0 + gamma) * yp - gamma * yo) + w0 * y0[r];
+        if (write_cand) yc[r] = yp;
+    }
+};
+
+struct EpiBStore {
+    double* out;
+    const int* inst;
+    const int* done;
+    __device__ bool active() const { return true; }
+    __device__ bool skip_rows(int r0, int r1) const { return !any_active(done, inst, r0, r1); }
+    __device__ void operator()(int r, double s) const {
+        if (!done[inst[r]]) out[r] = s;
+    }
+};
+
+struct EpiStorePlain {
+    double* out;
+    __device__ bool active() const { return true; }
+    __device__ void operator()(int r, double s) const { out[r] = s; }
+};
+
+__device__ __forceinline__ bool lo_fin(double l) { return l > -1e20; }
+__device__ __forceinline__ bool up_fin(double u) { return u < 1e20; }
+
+// One CTA per instance: the same KKT terms as the single-LP row / column passes.
+__global__ void __launch_bounds__(kThreads)
+k_bkkt(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const double* __restrict__ ax,
+       const double* __restrict__ aty, const double* __restrict__ xc, const double* __restrict__ yc,
+       const double* __restrict__ rl_s, const double* __restrict__ ru_s, const double* __restrict__ rl_o,
+       const double* __restrict__ ru_o, const double* __restrict__ rs, const double* __restrict__ c_s,
+       const double* __restrict__ cl_o, const double* __restrict__ cu_o, const double* __restrict__ cs,
+       const double* __restrict__ x_last, const double* __restrict__ y_last, double* __restrict__ part,
+       BatchArrays S) {
+    const int inst = blockIdx.x;
+    if (S.done[inst]) return;
+    __shared__ double red[kBQ * 32];
+    double v[kBQ] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // 0 rp_o^2, 1 rp_s^2, 2 dobj rows, 3 dy^2, 4 rd_o^2, 5 rd_s^2, 6 pobj, 7 dobj cols, 8 dx^2, 9 nan
+    for (int64_t i = roff[inst] + threadIdx.x; i < roff[inst + 1]; i += blockDim.x) {
+        const double a = ax[i], ys = yc[i];
+        if (!isfinite(a) || !isfinite(ys)) v[9] = 1.0;
+        const double ps = a - fmin(fmax(a, rl_s[i]), ru_s[i]);
+        const double ao = a / rs[i];
+        const double po = ao - fmin(fmax(ao, rl_o[i]), ru_o[i]);
+        const double yo = -ys * rs[i];
+        double dt = 0.0;
+        if (yo > 0.0 && lo_fin(rl_o[i])) dt = yo * rl_o[i];
+        else if (yo < 0.0 && up_fin(ru_o[i])) dt = yo * ru_o[i];
+        const double dy = ys - y_last[i];
+        v[0] += po * po; v[1] += ps * ps; v[2] += dt; v[3] += dy * dy;
+    }
+    for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x) {
+        const double at = aty[j], xs = xc[j];
+        if (!isfinite(at) || !isfinite(xs)) v[9] = 1.0;
+        const bool lf = lo_fin(cl_o[j]), uf = up_fin(cu_o[j]);
+        const double r_s = c_s[j] + at, r_o = r_s / cs[j];
+        auto lam_of = [&](double r) { return (lf && uf) ? r : lf ? fmax(r, 0.0) : uf ? fmin(r, 0.0) : 0.0; };
+        const double lo = lam_of(r_o), ls = lam_of(r_s);
+        double dt = 0.0;
+        if (lo > 0.0) dt = lo * cl_o[j];
+        else if (lo < 0.0) dt = lo * cu_o[j];
+        const double dx = xs - x_last[j];
+        v[4] += (r_o - lo) * (r_o - lo); v[5] += (r_s - ls) * (r_s - ls);
+        v[6] += c_s[j] * xs; v[7] += dt; v[8] += dx * dx;
+    }
+    double f[1] = {v[9]};
+    block_reduce<OpSum, double, kBQ - 1>(*reinterpret_cast<double(*)[kBQ - 1]>(v), red);
+    block_reduce<OpMax, double, 1>(f, red);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < kBQ - 1; ++q) part[inst * kBQ + q] = v[q];
+        part[inst * kBQ + kBQ - 1] = f[0];
+    }
+}
+
+struct BControl {
+    double tol, beta_sufficient, beta_necessary, beta_artificial, pw_smoothing;
+    int len, count;
+};
+
+// One thread per instance: the single-LP control rules (halpern_mode.cu) per instance.
+__global__ void k_bcontrol(const double* __restrict__ part, BControl cp, BatchArrays S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cp.count || S.done[i]) return;
+    const double* s = part + i * kBQ;
+    S.total[i] += cp.len;
+    S.restart_flag[i] = 0;
+    if (s[9] > 0.0 || isnan(s[0]) || isnan(s[4])) {
+        S.done[i] = 1;
+        S.status[i] = 9;
+        return;
+    }
+    const double pobj = s[6] + S.offset_min[i];
+    const double dobj = s[2] + s[7] + S.offset_min[i];
+    const double rel_p = sqrt(s[0]) / (1.0 + S.bnorm[i]);
+    const double rel_d = sqrt(s[4]) / (1.0 + S.cnorm[i]);
+    const double gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    const double rel = fmax(rel_p, fmax(rel_d, gap));
+    S.rel_p[i] = rel_p; S.rel_d[i] = rel_d; S.rel_gap[i] = gap; S.rel_kkt[i] = rel;
+    S.pobj[i] = pobj; S.dobj[i] = dobj;
+    if (rel <= cp.tol) {
+        S.done[i] = 1;
+        S.status[i] = 1;
+        return;
+    }
+    const double omega = S.omega[i];
+    const double wk = sqrt(omega * s[1] + s[5] / omega + gap * gap);
+    if (S.kkt_start[i] < 0.0) { S.kkt_start[i] = wk; S.kkt_prev[i] = wk; }
+    const long long k_in = S.k_base[i] + cp.len;
+    const bool restart = (wk <= cp.beta_sufficient * S.kkt_start[i]) ||
+                         (wk <= cp.beta_necessary * S.kkt_start[i] && wk > S.kkt_prev[i]) ||
+                         (static_cast<double>(k_in) >= cp.beta_artificial * static_cast<double>(S.total[i]));
+    S.kkt_prev[i] = wk;
+    if (restart) {
+        const double dx = sqrt(s[8]), dy = sqrt(s[3]);
+        if (dx > 1e-10 && dy > 1e-10) {
+            const double th = cp.pw_smoothing;
+            S.omega[i] = exp(th * log(dy / dx) + (1.0 - th) * log(omega));
+            S.tau[i] = S.eta[i] / S.omega[i];
+            S.sigma[i] = S.eta[i] * S.omega[i];
+        }
+        S.k_base[i] = 0;
+        S.kkt_start[i] = wk;
+        S.kkt_prev[i] = wk;
+        S.restart_count[i] += 1;
+        S.restart_flag[i] = 1;
+    } else {
+        S.k_base[i] = k_in;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restrict__ done, BatchCounters* out) {
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    for (int i = threadIdx.x; i < count; i += blockDim.x) v[0] += done[i] ? 0.0 : 1.0;
+    block_reduce<OpSum, double, 1>(v, red);
+    if (threadIdx.x == 0) out->active = static_cast<int>(v[0]);
+}
+
+__global__ void k_brestart(int m, int n, const int* __restrict__ row_inst, const int* __restrict__ col_inst,
+                           const double* __restrict__ xc, const double* __restrict__ yc, double* __restrict__ x,
+                           double* __restrict__ x0, double* __restrict__ y, double* __restrict__ y0,
+                           double* __restrict__ x_last, double* __restrict__ y_last, BatchArrays S) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n && S.restart_flag[col_inst[t]]) { const double v = xc[t]; x[t] = v; x0[t] = v; x_last[t] = v; }
+    if (t < m && S.restart_flag[row_inst[t]]) { const double v = yc[t]; y[t] = v; y0[t] = v; y_last[t] = v; }
+}
+
+// Per-instance norms (||b||, ||c|| original; ||b||, ||c|| scaled) and initial state.
+__global__ void __launch_bounds__(kThreads)
+k_binit(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const double* __restrict__ rl_o,
+        const double* __restrict__ ru_o, const double* __restrict__ c_o, const double* __restrict__ rl_s,
+        const double* __restrict__ ru_s, const double* __restrict__ c_s, const int* __restrict__ sense,
+        const double* __restrict__ offsets, double step_safety, BatchArrays S) {
+    const int inst = blockIdx.x;
+    __shared__ double red[4 * 32];
+    double v[4] = {0, 0, 0, 0};
+    auto b2 = [](double l, double u) {
+        const bool lf = l > -1e20, uf = u < 1e20;
+        if (lf && uf && l == u) return l * l;
+        return (lf ? l * l : 0.0) + (uf ? u * u : 0.0);
+    };
+    for (int64_t i = roff[inst] + threadIdx.x; i < roff[inst + 1]; i += blockDim.x) {
+        v[0] += b2(rl_o[i], ru_o[i]);
+        v[2] += b2(rl_s[i], ru_s[i]);
+    }
+    for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x) {
+        v[1] += c_o[j] * c_o[j];
+        v[3] += c_s[j] * c_s[j];
+    }
+    block_reduce<OpSum, double, 4>(v, red);
+    if (threadIdx.x != 0) return;
+    const double bn = sqrt(v[0]), cn = sqrt(v[1]), bs = sqrt(v[2]), csn = sqrt(v[3]);
+    const double norm = S.lambda[inst] > 1e-12 ? S.lambda[inst] : 1.0;
+    const double eta = step_safety / norm;
+    const double omega = (bs > 1e-10 && csn > 1e-10) ? csn / bs : 1.0;
+    S.bnorm[inst] = bn; S.cnorm[inst] = cn;
+    S.eta[inst] = eta; S.omega[inst] = omega; S.tau[inst] = eta / omega; S.sigma[inst] = eta * omega;
+    S.kkt_start[inst] = -1.0; S.kkt_prev[inst] = -1.0;
+    S.offset_min[inst] = sense[inst] ? -offsets[inst] : offsets[inst];
+    S.k_base[inst] = 0; S.total[inst] = 0;
+    S.done[inst] = 0; S.status[inst] = 0; S.restart_count[inst] = 0; S.restart_flag[inst] = 0;
+    S.rel_kkt[inst] = 1e30;
+}
+
+__global__ void k_binit_iterates(int m, int n, const double* __restrict__ cl, const double* __restrict__ cu,
+                                 double* x, double* x0, double* xb, double* xc, double* x_last,
+                                 double* y, double* y0, double* yc, double* y_last) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        const double v = fmin(fmax(0.0, cl[t]), cu[t]);
+        x[t] = x0[t] = xb[t] = xc[t] = x_last[t] = v;
+    }
+    if (t < m) { y[t] = y0[t] = yc[t] = y_last[t] = 0.0; }
+}
+
+// Batched power iteration, one CTA per instance: ||u_i||, then v_i = u_i / ||u_i||.
+__global__ void __launch_bounds__(kThreads)
+k_bpower(const int64_t* __restrict__ coff, const double* __restrict__ u, double* __restrict__ v, BatchArrays S) {
+    const int inst = blockIdx.x;
+    __shared__ double red[32];
+    __shared__ double inv;
+    double s[1] = {0.0};
+    for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x) s[0] += u[j] * u[j];
+    block_reduce<OpSum, double, 1>(s, red);
+    if (threadIdx.x == 0) {
+        const double nrm = sqrt(s[0]);
+        S.lambda[inst] = sqrt(nrm);                 // sigma_max estimate = sqrt(||A^T A v||)
+        inv = nrm > 1e-300 ? 1.0 / nrm : 0.0;
+    }
+    __syncthreads();
+    for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x) v[j] = u[j] * inv;
+}
+
+__global__ void k_bpower_init(int n, const int* __restrict__ col_inst, const int64_t* __restrict__ coff,
+                              double* __restrict__ v) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int i = col_inst[j];
+    v[j] = 1.0 / sqrt(static_cast<double>(coff[i + 1] - coff[i]));
+}
+
+__global__ void k_bpost(int m, int n, const int* __restrict__ col_inst, const int* __restrict__ sense,
+                        const double* __restrict__ xc, const double* __restrict__ yc, const double* __restrict__ cs,
+                        const double* __restrict__ rs, int scaled, double* __restrict__ x_out,
+                        double* __restrict__ y_out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) x_out[t] = scaled ? xc[t] * cs[t] : xc[t];
+    if (t < m) y_out[t] = -(scaled ? yc[t] * rs[t] : yc[t]);
+    (void)col_inst; (void)sense;
+}
+
+__global__ void k_breduced(int n, const int* __restrict__ col_inst, const int* __restrict__ sense,
+                           const double* __restrict__ c, double* __restrict__ d) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) d[j] = sense[col_inst[j]] ? c[j] + d[j] : c[j] - d[j];
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_bobjective(const int64_t* __restrict__ coff, const double* __restrict__ c, const double* __restrict__ x,
+             const double* __restrict__ offsets, double* __restrict__ out) {
+    const int inst = blockIdx.x;
+    __shared__ double red[32];
+    double s[1] = {0.0};
+    for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x) s[0] += c[j] * x[j];
+    block_reduce<OpSum, double, 1>(s, red);
+    if (threadIdx.x == 0) out[inst] = offsets[inst] + s[0];
+}
+
+__global__ void k_fill_inst(int64_t total, const int64_t* __restrict__ off, int count, int* __restrict__ inst) {
+    const int i = blockIdx.x;   // one CTA per instance
+    if (i >= count) return;
+    for (int64_t t = off[i] + threadIdx.x; t < off[i + 1]; t += blockDim.x) inst[t] = i;
+    (void)total;
+}
+
+template <typename T>
+vajra_status up(DeviceBuffer<T>& d, const std::vector<T>& h, cudaStream_t st) {
+    VJ_TRY(d.alloc(h.size()));
+    if (!h.empty()) VJ_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return VAJRA_OK;
+}
+
+}  // namespace
+
+vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajra_result* results,
+                       cudaStream_t st, double* device_time) {
+    const auto t_start = Clock::now();
+    // ---- host packing (block-diagonal CSC) ----------------------------------------------
+    std::vector<int64_t> roff(count + 1, 0), coff(count + 1, 0), zoff(count + 1, 0);
+    for (int i = 0; i < count; ++i) {
+        roff[i + 1] = roff[i] + lps[i].num_rows;
+        coff[i + 1] = coff[i] + lps[i].num_cols;
+        zoff[i + 1] = zoff[i] + lps[i].nnz;
+    }
+    const int64_t M = roff[count], N = coff[count], NNZ = zoff[count];
+    if (M >= (1LL << 31) || N >= (1LL << 31)) { set_error("packed batch exceeds 2^31 rows or columns"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    const int m = static_cast<int>(M), n = static_cast<int>(N);
+    vajra_lp packed{};
+    std::vector<int64_t> cp(n + 1);
+    std::vector<int32_t> ri(NNZ);
+    std::vector<double> vals(NNZ), c(n), cl(n), cu(n), rl(m), ru(m), offsets(count);
+    std::vector<int> sense(count);
+    for (int i = 0; i < count; ++i) {
+        const vajra_lp& L = lps[i];
+        const int64_t c0 = coff[i], r0 = roff[i], z0 = zoff[i];
+        for (int j = 0; j < L.num_cols; ++j) cp[c0 + j] = z0 + L.col_ptr[j];
+        for (int64_t k = 0; k < L.nnz; ++k) ri[z0 + k] = static_cast<int32_t>(r0 + L.row_idx[k]);
+        if (L.nnz) std::memcpy(&vals[z0], L.values, sizeof(double) * L.nnz);
+        if (L.num_cols) {
+            std::memcpy(&c[c0], L.c, sizeof(double) * L.num_cols);
+            std::memcpy(&cl[c0], L.col_lower, sizeof(double) * L.num_cols);
+            std::memcpy(&cu[c0], L.col_upper, sizeof(double) * L.num_cols);
+        }
+        if (L.num_rows) {
+            std::memcpy(&rl[r0], L.row_lower, sizeof(double) * L.num_rows);
+            std::memcpy(&ru[r0], L.row_upper, sizeof(double) * L.num_rows);
+        }
+        sense[i] = L.sense;
+        offsets[i] = L.objective_offset;
+    }
+    cp[n] = NNZ;
+    packed.num_rows = m; packed.num_cols = n; packed.nnz = NNZ;
+    packed.col_ptr = cp.data(); packed.row_idx = ri.data(); packed.values = vals.data();
+    packed.c = c.data(); packed.col_lower = cl.data(); packed.col_upper = cu.data();
+    packed.row_lower = rl.data(); packed.row_upper = ru.data();
+    // maximisation instances are negated here (the packed problem is a minimisation)
+    std::vector<double> cmin(c);
+    for (int i = 0; i < count; ++i)
+        if (sense[i]) for (int64_t j = coff[i]; j < coff[i + 1]; ++j) cmin[j] = -cmin[j];
+
+    StreamTimer timer;
+    timer.start(st);
+    DeviceLp lp;
+    VJ_TRY(upload_lp(&packed, lp, st));
+    DeviceBuffer<double> d_cmin;
+    VJ_TRY(up(d_cmin, cmin, st));
+    DeviceBuffer<int64_t> d_roff, d_coff;
+    DeviceBuffer<int> d_sense, row_inst, col_inst;
+    DeviceBuffer<double> d_offsets;
+    VJ_TRY(up(d_roff, roff, st));
+    VJ_TRY(up(d_coff, coff, st));
+    VJ_TRY(up(d_sense, sense, st));
+    VJ_TRY(up(d_offsets, offsets, st));
+    VJ_TRY(row_inst.alloc(m));
+    VJ_TRY(col_inst.alloc(n));
+    k_fill_inst<<<count, kThreads, 0, st>>>(M, d_roff.get(), count, row_inst.get());
+    k_fill_inst<<<count, kThreads, 0, st>>>(N, d_coff.get(), count, col_inst.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(2);
+
+    // ---- set-up on the packed problem --------------------------------------------------
+    Prepared p;
+    DeviceBuffer<SetupState> sst;
+    VJ_TRY(sst.alloc(1));
+    VJ_TRY(build_csr(lp, p, st));
+    ScalingOpts so;
+    so.enable = o.enable_scaling != 0;
+    so.ruiz_iterations = o.ruiz_iterations > 0 ? o.ruiz_iterations : 10;
+    so.pock_chambolle = o.pock_chambolle != 0;
+    so.negate_c = false;
+    {
+        // Upload the min-form c as the raw c for scaling, keep the caller's c for reporting.
+        DeviceBuffer<double> c_raw;
+        std::swap(c_raw, lp.c);
+        std::swap(lp.c, d_cmin);
+        VJ_TRY(prepare_scaled(lp, p, so, sst.get(), st));
+        std::swap(d_cmin, lp.c);
+        std::swap(lp.c, c_raw);   // lp.c = caller's c again, d_cmin = min-form c
+    }
+    VJ_TRY(plan_spmv(lp, p, st));
+
+    // ---- per-instance state -------------------------------------------------------------
+    DeviceBuffer<double> dd;
+    DeviceBuffer<long long> dl;
+    DeviceBuffer<int> di;
+    VJ_TRY(dd.alloc(16 * static_cast<size_t>(count)));
+    VJ_TRY(dl.alloc(2 * static_cast<size_t>(count)));
+    VJ_TRY(di.alloc(4 * static_cast<size_t>(count)));
+    BatchArrays S;
+    double** fields[] = {&S.omega, &S.eta, &S.tau, &S.sigma, &S.kkt_start, &S.kkt_prev, &S.rel_p, &S.rel_d,
+                         &S.rel_gap, &S.rel_kkt, &S.pobj, &S.dobj, &S.bnorm, &S.cnorm, &S.offset_min, &S.lambda};
+    for (int q = 0; q < 16; ++q) *fields[q] = dd.get() + static_cast<size_t>(q) * count;
+    S.k_base = dl.get(); S.total = dl.get() + count;
+    S.done = di.get(); S.status = di.get() + count; S.restart_count = di.get() + 2 * count;
+    S.restart_flag = di.get() + 3 * count;
+    VJ_CUDA(cudaMemsetAsync(di.get(), 0, sizeof(int) * 4 * count, st));   // done = 0 for the power iteration
+
+    // batched power iteration (fixed 60 rounds)
+    {
+        DeviceBuffer<double> v, w, u;
+        VJ_TRY(v.alloc(n));
+        VJ_TRY(w.alloc(m));
+        VJ_TRY(u.alloc(n));
+        k_bpower_init<<<grid_for(n), kThreads, 0, st>>>(n, col_inst.get(), d_coff.get(), v.get());
+        note_launch(1);
+        for (int it = 0; it < 60; ++it) {
+            launch_spmv_t<double, double, double>(p.a, p.csr_val.get(), v.get(), EpiStorePlain{w.get()}, st);
+            launch_spmv_t<double, double, double>(p.at, p.csc_val.get(), w.get(), EpiStorePlain{u.get()}, st);
+            k_bpower<<<count, kThreads, 0, st>>>(d_coff.get(), u.get(), v.get(), S);
+            note_launch(1);
+        }
+        VJ_LAUNCH_CHECK();
+        VJ_CUDA(cudaStreamSynchronize(st));
+    }
+    const double safety = (o.step_safety > 0.0 && o.step_safety < 1.0) ? o.step_safety : 0.99;
+    k_binit<<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), lp.row_lower.get(), lp.row_upper.get(), d_cmin.get(),
+                                        p.row_lower.get(), p.row_upper.get(), p.c.get(), d_sense.get(), d_offsets.get(),
+                                        safety, S);
+    note_launch(1);
+
+    // iterates
+    DeviceBuffer<double> x, x0, xb, xc, y, y0, yc, x_last, y_last, ax, aty, part;
+    for (auto* b : {&x, &x0, &xb, &xc, &x_last, &aty}) VJ_TRY(b->alloc(n));
+    for (auto* b : {&y, &y0, &yc, &y_last, &ax}) VJ_TRY(b->alloc(m));
+    VJ_TRY(part.alloc(static_cast<size_t>(count) * kBQ));
+    const int mx = m > n ? m : n;
+    k_binit_iterates<<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), x.get(), x0.get(),
+                                                        xb.get(), xc.get(), x_last.get(), y.get(), y0.get(), yc.get(),
+                                                        y_last.get());
+    note_launch(1);
+    VJ_LAUNCH_CHECK();
+
+    // autotune the packed SpMVs (store epilogue, no skipping)
+    CsrView a = p.a, at = p.at;
+    if (o.autotune) {
+        cudaEvent_t e0, e1;
+        VJ_CUDA(cudaEventCreate(&e0));
+        VJ_CUDA(cudaEventCreate(&e1));
+        for (CsrView* v : {&a, &at}) {
+            const double* xin = (v == &a) ? xb.get() : y.get();
+            double* out = (v == &a) ? ax.get() : aty.get();
+            const double* val = (v == &a) ? p.csr_val.get() : p.csc_val.get();
+            float best = 1e30f;
+            int best_g = v->group;
+            for (int g : {0, 1, 2, 4, 8, 16, 32}) {
+                CsrView t = *v;
+                t.group = g;
+                launch_spmv_t<double, double, double>(t, val, xin, EpiStorePlain{out}, st);
+                VJ_CUDA(cudaEventRecord(e0, st));
+                for (int r = 0; r < 3; ++r) launch_spmv_t<double, double, double>(t, val, xin, EpiStorePlain{out}, st);
+                VJ_CUDA(cudaEventRecord(e1, st));
+                VJ_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                VJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best) { best = ms; best_g = g; }
+            }
+            v->group = best_g;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+
+    DeviceBuffer<BatchCounters> counters;
+    VJ_TRY(counters.alloc(1));
+    BatchCounters* hc = nullptr;
+    VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hc), sizeof(BatchCounters)));
+    struct Guard {
+        BatchCounters* h; cudaGraph_t g = nullptr; cudaGraphExec_t e = nullptr;
+        ~Guard() { if (e) cudaGraphExecDestroy(e); if (g) cudaGraphDestroy(g); if (h) cudaFreeHost(h); }
+    } guard{hc};
+
+    BControl bc{};
+    bc.tol = o.tolerance;
+    bc.beta_sufficient = o.restart_sufficient;
+    bc.beta_necessary = o.restart_necessary;
+    bc.beta_artificial = o.restart_artificial;
+    bc.pw_smoothing = o.primal_weight_smoothing;
+    bc.count = count;
+    const double gamma = o.reflection;
+    const int K = o.check_frequency > 0 ? o.check_frequency : 64;
+    int64_t graph_kernels = 0;
+
+    auto enqueue_chunk = [&](int len) {
+        for (int kk = 0; kk < len; ++kk) {
+            const int wc = kk == len - 1 ? 1 : 0;
+            launch_spmv_t<double, double, double>(
+                at, p.csc_val.get(), y.get(),
+                EpiBPrimal{p.c.get(), p.col_lower.get(), p.col_upper.get(), x0.get(), x.get(), xb.get(), xc.get(),
+                           col_inst.get(), S, gamma, kk, wc}, st);
+            launch_spmv_t<double, double, double>(
+                a, p.csr_val.get(), xb.get(),
+                EpiBDual{p.row_lower.get(), p.row_upper.get(), y0.get(), y.get(), yc.get(), row_inst.get(), S, gamma,
+                         kk, wc}, st);
+        }
+        launch_spmv_t<double, double, double>(a, p.csr_val.get(), xc.get(), EpiBStore{ax.get(), row_inst.get(), S.done}, st);
+        launch_spmv_t<double, double, double>(at, p.csc_val.get(), yc.get(), EpiBStore{aty.get(), col_inst.get(), S.done}, st);
+        k_bkkt<<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), ax.get(), aty.get(), xc.get(), yc.get(),
+                                           p.row_lower.get(), p.row_upper.get(), lp.row_lower.get(), lp.row_upper.get(),
+                                           p.row_scale.get(), p.c.get(), lp.col_lower.get(), lp.col_upper.get(),
+                                           p.col_scale.get(), x_last.get(), y_last.get(), part.get(), S);
+        BControl c2 = bc;
+        c2.len = len;
+        k_bcontrol<<<(count + 127) / 128, 128, 0, st>>>(part.get(), c2, S);
+        k_brestart<<<grid_for(mx), kThreads, 0, st>>>(m, n, row_inst.get(), col_inst.get(), xc.get(), yc.get(), x.get(),
+                                                      x0.get(), y.get(), y0.get(), x_last.get(), y_last.get(), S);
+        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get());
+        note_launch(4);
+    };
+
+    const int64_t max_iter = o.iteration_limit;
+    int64_t launched = 0;
+    bool time_out = false;
+    while (launched < max_iter) {
+        const int64_t remaining = max_iter - launched;
+        const int len = static_cast<int>(remaining < K ? remaining : K);
+        if (len == K) {
+            if (!guard.e) {
+                const int64_t before = launch_count();
+                VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                enqueue_chunk(len);
+                VJ_CUDA(cudaStreamEndCapture(st, &guard.g));
+                VJ_CUDA(cudaGraphInstantiate(&guard.e, guard.g, 0));
+                graph_kernels = launch_count() - before;
+                launch_count() = before;
+            }
+            VJ_CUDA(cudaGraphLaunch(guard.e, st));
+            note_launch(graph_kernels);
+        } else {
+            enqueue_chunk(len);
+            VJ_LAUNCH_CHECK();
+        }
+        launched += len;
+        VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+        VJ_CUDA(cudaStreamSynchronize(st));
+        if (hc->active == 0) break;
+        if (seconds_since(t_start) > o.time_limit) { time_out = true; break; }
+    }
+
+    // ---- post-processing -------------------------------------------------------------------
+    DeviceBuffer<double> x_out, y_out, row_value, col_dual, objs;
+    VJ_TRY(x_out.alloc(n));
+    VJ_TRY(y_out.alloc(m));
+    VJ_TRY(row_value.alloc(m));
+    VJ_TRY(col_dual.alloc(n));
+    VJ_TRY(objs.alloc(count));
+    k_bpost<<<grid_for(mx), kThreads, 0, st>>>(m, n, col_inst.get(), d_sense.get(), xc.get(), yc.get(),
+                                               p.col_scale.get(), p.row_scale.get(), p.scaled ? 1 : 0, x_out.get(),
+                                               y_out.get());
+    launch_spmv_t<double, double, double>(a, p.csr_val_orig.get(), x_out.get(), EpiStorePlain{row_value.get()}, st);
+    launch_spmv_t<double, double, double>(at, lp.values.get(), y_out.get(), EpiStorePlain{col_dual.get()}, st);
+    k_breduced<<<grid_for(n), kThreads, 0, st>>>(n, col_inst.get(), d_sense.get(), lp.c.get(), col_dual.get());
+    k_bobjective<<<count, kThreads, 0, st>>>(d_coff.get(), lp.c.get(), x_out.get(), d_offsets.get(), objs.get());
+    note_launch(3);
+    VJ_LAUNCH_CHECK();
+    timer.stop(st);
+    std::vector<double> hx(n), hy(m), hrv(m), hcd(n), hobj(count), hd(16 * static_cast<size_t>(count));
+    std::vector<long long> hl(2 * static_cast<size_t>(count));
+    std::vector<int> hi(4 * static_cast<size_t>(count));
+    VJ_CUDA(cudaMemcpyAsync(hx.data(), x_out.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hy.data(), y_out.get(), sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hrv.data(), row_value.get(), sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hcd.data(), col_dual.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hobj.data(), objs.get(), sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hd.data(), dd.get(), sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hl.data(), dl.get(), sizeof(long long) * hl.size(), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaMemcpyAsync(hi.data(), di.get(), sizeof(int) * hi.size(), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    if (device_time) *device_time = timer.seconds();
+    auto field = [&](int q, int i) { return hd[static_cast<size_t>(q) * count + i]; };
+    for (int i = 0; i < count; ++i) {
+        vajra_result* r = &results[i];
+        const int64_t r0 = roff[i], c0 = coff[i];
+        const int mi = lps[i].num_rows, ni = lps[i].num_cols;
+        if (r->col_value) std::memcpy(r->col_value, &hx[c0], sizeof(double) * ni);
+        if (r->col_dual) std::memcpy(r->col_dual, &hcd[c0], sizeof(double) * ni);
+        if (r->row_value) std::memcpy(r->row_value, &hrv[r0], sizeof(double) * mi);
+        if (r->row_dual) std::memcpy(r->row_dual, &hy[r0], sizeof(double) * mi);
+        const int status = hi[static_cast<size_t>(count) + i];
+        r->status = status ? status : (time_out ? 7 : 6);
+        r->iterations = hl[static_cast<size_t>(count) + i];
+        r->objective_value = hobj[i];
+        r->dual_objective = sense[i] ? -field(11, i) : field(11, i);
+        r->restart_count = hi[2 * static_cast<size_t>(count) + i];
+        r->rel_primal = r->primal_residual = field(6, i);
+        r->rel_dual = r->dual_residual = field(7, i);
+        r->rel_gap = r->duality_gap = field(8, i);
+        r->rel_kkt = field(9, i);
+        r->primal_weight = field(0, i);
+        r->tau = field(2, i);
+        r->sigma = field(3, i);
+        r->spectral_norm_estimate = field(15, i);
+        r->converged = r->status == 1 ? 1 : 0;
+        r->fp64_iterations = r->iterations;
+        r->fp32_iterations = 0;
+        r->spmv_group_a = a.group;
+        r->spmv_group_at = at.group;
+        std::snprintf(r->status_message, sizeof(r->status_message), "%s",
+                      r->status == 1 ? "relative KKT tolerance reached (batched)"
+                      : r->status == 9 ? "NaN/Inf in the KKT evaluation (batched)"
+                      : "limit reached before this instance converged (batched)");
+    }
+    return VAJRA_OK;
+}
+
+}  // namespace vajra

@@ -376,6 +376,52 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
     return s;
 }
 
+vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const vajra_opts* opts,
+                                    vajra_result* results) {
+    if (count <= 0 || !lps || !results) { set_error("empty batch or NULL arrays"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    const auto t0 = Clock::now();
+    for (int i = 0; i < count; ++i) {
+        vajra_status s = validate_host(&lps[i]);
+        if (s == VAJRA_OK && (lps[i].num_rows == 0 || lps[i].num_cols == 0)) {
+            set_error("instance %d has no rows or no columns (solve it with vajra_pdhg_solve)", i);
+            s = VAJRA_ERR_INVALID_ARGUMENT;
+        }
+        if (s != VAJRA_OK) {
+            for (int k = 0; k < count; ++k) fail_result(&results[k], s);
+            return s;
+        }
+    }
+    vajra_opts o;
+    if (opts) o = *opts; else vajra_default_opts(&o);
+    vajra_device_info info;
+    if (vajra_probe_device(o.device, &info) != VAJRA_OK) {
+        set_error("no usable CUDA device %d (no CPU fallback)", o.device);
+        for (int k = 0; k < count; ++k) fail_result(&results[k], VAJRA_ERR_NO_DEVICE);
+        return VAJRA_ERR_NO_DEVICE;
+    }
+    if (cudaSetDevice(o.device) != cudaSuccess) return cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__);
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__);
+    const int64_t launches0 = launch_count();
+    double dev_time = 0.0;
+    vajra_status s = run_batch(count, lps, o, results, st, &dev_time);
+    if (s != VAJRA_OK) {
+        for (int k = 0; k < count; ++k) fail_result(&results[k], s);
+        cudaGetLastError();
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    const double total = seconds_since(t0);
+    const int64_t launches = launch_count() - launches0;
+    for (int k = 0; k < count; ++k) {
+        results[k].total_time_sec = total;
+        results[k].device_time_sec = dev_time;
+        results[k].kernel_launches = launches;
+    }
+    return s;
+}
+
 // ---------------------------------------------------------------------------------------
 // kernel-level entry points
 // ---------------------------------------------------------------------------------------

@@ -48,6 +48,8 @@ struct StreamTimer {
 
 vajra_status run_reference(vajra_pdhg* h, vajra_result* r);
 vajra_status run_halpern(vajra_pdhg* h, vajra_result* r);
+vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajra_result* results,
+                       cudaStream_t st, double* device_time);
 
 // Closed forms for LPs without rows or without nonzeros (pdhg.cpp:88-127 for m = 0 / n = 0;
 // for nnz = 0 the rows decouple from the columns).  Returns true when it handled the LP.

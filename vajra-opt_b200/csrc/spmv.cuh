@@ -56,6 +56,17 @@ __device__ __forceinline__ T extrapolate_exact(T x_new, T x_old) {   // 2 x_new 
     return rn_sub(rn_mul(T(2), x_new), x_old);
 }
 
+// ----- optional row-skip hook ----------------------------------------------------------
+// An epilogue may define `bool skip_rows(int r0, int r1) const`: true when none of the rows
+// [r0, r1) needs a result (the batched solver's finished instances).  The kernels then skip
+// those rows' loads entirely.  Epilogues without the member never skip.
+template <class E>
+__device__ __forceinline__ auto skip_rows_impl(const E& e, int r0, int r1, int) -> decltype(e.skip_rows(r0, r1)) {
+    return e.skip_rows(r0, r1);
+}
+template <class E>
+__device__ __forceinline__ bool skip_rows_impl(const E&, int, int, long) { return false; }
+
 // ----- epilogues usable by both families ---------------------------------------------
 template <typename T>
 struct EpiStore {
@@ -97,6 +108,7 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
         // One CTA per long row.
         __shared__ Acc red[32];
         const int row = long_rows[blockIdx.x - vec_blocks];
+        if (skip_rows_impl(epi, row, row + 1, 0)) return;
         const int64_t s = ptr[row], e = ptr[row + 1];
         Acc acc = Acc(0);
         for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
@@ -113,7 +125,7 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
     if (valid) {
         s = ptr[row];
         e = ptr[row + 1];
-        if (e - s > long_len) valid = false;
+        if (e - s > long_len || skip_rows_impl(epi, row, row + 1, 0)) valid = false;
     }
     Acc acc = Acc(0);
     if (valid) {
@@ -167,6 +179,7 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
     if (!epi.active()) return;
     if (static_cast<int>(blockIdx.x) >= nb) {
         const int row = long_rows[blockIdx.x - nb];
+        if (skip_rows_impl(epi, row, row + 1, 0)) return;
         const int64_t s = ptr[row], e = ptr[row + 1];
         Acc acc = Acc(0);
         for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
@@ -180,6 +193,7 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
     if (r0 >= r1) return;
     int r_end = r1;
     if (ptr[r1] - ptr[r1 - 1] > kTile) r_end = r1 - 1;
+    if (r0 >= r_end || skip_rows_impl(epi, r0, r_end, 0)) return;
     const int64_t e0 = ptr[r0], e1 = ptr[r_end];
     for (int64_t q = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x); q < e1; q += 4 * blockDim.x) {
         int ii[4];

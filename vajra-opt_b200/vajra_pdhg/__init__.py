@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "NOT_SOLVED", 1: "OPTIMAL", 2: "INFEASIBLE", 3: "UNBOUNDED",
                 7: "TIME_LIMIT", 8: "NODE_LIMIT", 9: "NUMERICAL_ERROR", 10: "MODEL_ERROR",
                 11: "UNSUPPORTED"}
 
-__all__ = ["solve", "Solver", "default_opts", "probe_device", "is_cuda_available",
+__all__ = ["solve", "solve_batch", "Solver", "default_opts", "probe_device", "is_cuda_available",
            "last_timing", "ALGO_REFERENCE", "ALGO_HALPERN", "PREC_FP64", "PREC_MIXED",
            "STATUS_NAMES"]
 
@@ -87,6 +87,25 @@ def solve(lp, **opts) -> dict:
     if st != _capi.OK:
         raise RuntimeError(f"vajra_pdhg_solve failed ({st}): {res['status_message']}")
     return res
+
+
+def solve_batch(lps, **opts) -> list:
+    """Many independent LPs in one call (vajra_pdhg_solve_batch): packed block-diagonally on
+    the device, per-instance restarts and termination.  Returns one result dict per LP."""
+    hosts = [_HostLp(lp) for lp in lps]
+    arr = (_capi.VajraLp * len(lps))(*[h.s for h in hosts])
+    res = (_capi.VajraResult * len(lps))()
+    outs = []
+    for i, lp in enumerate(lps):
+        r, out = _alloc(lp)
+        res[i] = r
+        outs.append(out)
+    o = default_opts(**opts)
+    st = _capi.lib().vajra_pdhg_solve_batch(len(lps), arr, C.byref(o), res)
+    results = [_result_dict(res[i], outs[i]) for i in range(len(lps))]
+    if st != _capi.OK:
+        raise RuntimeError(f"vajra_pdhg_solve_batch failed ({st}): {results[0]['status_message']}")
+    return results
 
 
 class Solver:

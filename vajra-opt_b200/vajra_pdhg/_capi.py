@@ -87,6 +87,7 @@ SIGNATURES = [
     ("vajra_default_opts", None, [C.POINTER(VajraOpts)]),
     ("vajra_pdhg_solve", C.c_int32, [C.POINTER(VajraLp), C.POINTER(VajraOpts), C.POINTER(VajraResult)]),
     ("vajra_pdhg_create", C.c_int32, [C.POINTER(VajraLp), C.POINTER(VajraOpts), C.POINTER(C.c_void_p)]),
+    ("vajra_pdhg_solve_batch", C.c_int32, [C.c_int32, C.POINTER(VajraLp), C.POINTER(VajraOpts), C.POINTER(VajraResult)]),
     ("vajra_pdhg_run", C.c_int32, [C.c_void_p, C.POINTER(VajraResult)]),
     ("vajra_pdhg_destroy", C.c_int32, [C.c_void_p]),
     ("vajra_probe_device", C.c_int32, [C.c_int32, C.POINTER(VajraDeviceInfo)]),
