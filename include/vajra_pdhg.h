@@ -27,6 +27,10 @@
 extern "C" {
 #endif
 
+/* Layout version of the structs below.  A caller compiled against one version must not call
+ * a library of another: compare with vajra_abi_version() before the first call. */
+#define VAJRA_ABI_VERSION 3
+
 typedef int32_t vajra_status;
 enum {
     VAJRA_OK = 0,
@@ -117,7 +121,9 @@ typedef struct vajra_opts {
     double restart_artificial;  /* ... or inner iterations >= this x total (0.36)        */
     double primal_weight_smoothing; /* theta of omega <- exp(theta log(dy/dx) + (1-theta) log omega) (0.5) */
     double step_safety;         /* eta = step_safety / ||A||_2 (0.99)                    */
-    int32_t reserved[6];
+    int32_t restart_metric;     /* 0: primal-weighted KKT of T(z); 1: fixed-point residual
+                                   sqrt(omega ||x+ - x||^2 + ||y+ - y||^2 / omega)          */
+    int32_t reserved[5];
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and
@@ -232,6 +238,33 @@ vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const va
 vajra_status vajra_pdhg_run(vajra_pdhg* handle, vajra_result* result);
 vajra_status vajra_pdhg_destroy(vajra_pdhg* handle);
 
+/* ---- differentiation: adjoint of the unrolled PDHG map ---------------------------
+ * No counterpart in the reference (it has no derivatives); the forward map is the plain
+ * PDHG iteration of src/solvers/pdhg/pdhg.cpp:196-241 (primal first, fixed steps
+ * tau = sigma = step_safety / ||A_i||_2 after Ruiz + Pock-Chambolle scaling). */
+typedef struct vajra_unrolled_opts {
+    int32_t iterations;         /* unrolled iterations K (2000)                          */
+    int32_t checkpoint_every;   /* forward checkpoint interval (100); segments between
+                                   checkpoints are recomputed in the reverse pass         */
+    int32_t precision;          /* VAJRA_PREC_MIXED: FP32 map; VAJRA_PREC_FP64: FP64 map  */
+    int32_t enable_scaling;     /* Ruiz + Pock-Chambolle (constants of A)                */
+    double step_safety;         /* 0.95                                                   */
+    int32_t device;
+    int32_t reserved[5];
+} vajra_unrolled_opts;
+
+void vajra_default_unrolled_opts(vajra_unrolled_opts* opts);
+
+/* `count` minimisation LPs; vectors are packed over the instances in order (N = sum n_i,
+ * M = sum m_i).  Loss of instance i: sum_j (weights_j + c_j) x_j(K), x(K) in original units.
+ * loss[count] and x_final[N] are outputs (x_final may be NULL); grad_c[N],
+ * grad_row_lower[M], grad_row_upper[M] (any may be NULL; all NULL = forward only) receive
+ * dL_i/d(c, row_lower, row_upper) of the unrolled map (an equality row's right-hand side
+ * gradient is grad_row_lower + grad_row_upper). */
+vajra_status vajra_pdhg_unrolled(int32_t count, const vajra_lp* lps, const vajra_unrolled_opts* opts,
+                                 const double* weights, double* loss, double* x_final, double* grad_c,
+                                 double* grad_row_lower, double* grad_row_upper);
+
 /* ---- device probe and telemetry ------------------------------------------------ */
 
 /* Replaces indus::gpu::probe_device (gpu.hpp:49; gpu_context.cpp:16-59). */
@@ -243,6 +276,8 @@ int32_t vajra_is_cuda_available(void);
 void vajra_last_timing(vajra_timing* out);
 /* Human-readable text for a vajra_status. */
 const char* vajra_status_string(vajra_status status);
+/* VAJRA_ABI_VERSION the library was built with (no counterpart in the reference). */
+int32_t vajra_abi_version(void);
 
 /* ---- kernel-level entry points (device pointers, caller's stream; NULL = default) --
  * Each mirrors one kernel of src/solvers/gpu/spmv_kernels.cuh; the _f32 forms are the

@@ -152,6 +152,8 @@ using namespace vajra;
 
 extern "C" {
 
+int32_t vajra_abi_version(void) { return VAJRA_ABI_VERSION; }
+
 const char* vajra_status_string(vajra_status s) {
     switch (s) {
         case VAJRA_OK: return "ok";
@@ -373,6 +375,48 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
     vajra_pdhg_destroy(h);
     r->total_time_sec = seconds_since(t0);
     g_last_timing.total_time_sec = r->total_time_sec;
+    return s;
+}
+
+void vajra_default_unrolled_opts(vajra_unrolled_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->iterations = 2000;
+    o->checkpoint_every = 100;
+    o->precision = VAJRA_PREC_MIXED;
+    o->enable_scaling = 1;
+    o->step_safety = 0.95;
+    o->device = 0;
+}
+
+vajra_status vajra_pdhg_unrolled(int32_t count, const vajra_lp* lps, const vajra_unrolled_opts* opts,
+                                 const double* weights, double* loss, double* x_final, double* grad_c,
+                                 double* grad_row_lower, double* grad_row_upper) {
+    if (count <= 0 || !lps || !loss) { set_error("empty batch or NULL arrays"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    for (int i = 0; i < count; ++i) {
+        vajra_status s = validate_host(&lps[i]);
+        if (s == VAJRA_OK && (lps[i].num_rows == 0 || lps[i].num_cols == 0)) {
+            set_error("instance %d has no rows or no columns", i);
+            s = VAJRA_ERR_INVALID_ARGUMENT;
+        }
+        if (s != VAJRA_OK) return s;
+    }
+    vajra_unrolled_opts o;
+    if (opts) o = *opts; else vajra_default_unrolled_opts(&o);
+    if (o.iterations < 0) { set_error("negative iteration count"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    vajra_device_info info;
+    if (vajra_probe_device(o.device, &info) != VAJRA_OK) {
+        set_error("no usable CUDA device %d (no CPU fallback)", o.device);
+        return VAJRA_ERR_NO_DEVICE;
+    }
+    if (cudaSetDevice(o.device) != cudaSuccess) return cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__);
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__);
+    vajra_status s = run_unrolled(count, lps, o, weights, loss, x_final, grad_c, grad_row_lower, grad_row_upper, st);
+    if (s != VAJRA_OK) cudaGetLastError();
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
     return s;
 }
 

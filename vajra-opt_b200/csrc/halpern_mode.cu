@@ -23,7 +23,7 @@
 namespace vajra {
 namespace {
 
-constexpr int kQ = 6;             // partial sums per block in the check passes
+constexpr int kQ = 7;             // partial sums per block in the check passes (last: NaN flag)
 constexpr int kCheckBlocks = 148 * 4;
 constexpr int kHist = 16;
 
@@ -52,10 +52,12 @@ constexpr int kStatusIterLimit = 6;
 constexpr int kStatusTimeLimit = 7;
 constexpr int kStatusNumerical = 9;
 
+// At the last iteration of a chunk (write_cand) the epilogues also keep T(z) (xc, yc) and
+// the point it was taken from (xprev, yprev) for the check.
 template <typename T>
 struct EpiHPrimal {
     const T* c; const T* cl; const T* cu; const T* x0;
-    T* x; T* xb; T* xc;
+    T* x; T* xb; T* xc; T* xprev;
     const HState* st;
     double gamma;
     int kk, phase, write_cand;
@@ -72,14 +74,14 @@ struct EpiHPrimal {
         xp = xp < cl[j] ? cl[j] : (xp > cu[j] ? cu[j] : xp);
         xb[j] = xp + xp - xo;
         x[j] = w1 * ((T(1) + g) * xp - g * xo) + w0 * x0[j];
-        if (write_cand) xc[j] = xp;
+        if (write_cand) { xc[j] = xp; xprev[j] = xo; }
     }
 };
 
 template <typename T>
 struct EpiHDual {
     const T* rl; const T* ru; const T* y0;
-    T* y; T* yc;
+    T* y; T* yc; T* yprev;
     const HState* st;
     double gamma;
     int kk, phase, write_cand;
@@ -97,7 +99,7 @@ struct EpiHDual {
         q = q < rl[i] ? rl[i] : (q > ru[i] ? ru[i] : q);
         const T yp = yh - sigma * q;
         y[i] = w1 * ((T(1) + g) * yp - g * yo) + w0 * y0[i];
-        if (write_cand) yc[i] = yp;
+        if (write_cand) { yc[i] = yp; yprev[i] = yo; }
     }
 };
 
@@ -116,17 +118,19 @@ __device__ __forceinline__ bool finite_up(double u) { return u < 1e20; }
 // distance of y+ from the last restart point, NaN detection.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const double* __restrict__ rl_s,
-           const double* __restrict__ ru_s, const double* __restrict__ rl_o, const double* __restrict__ ru_o,
-           const double* __restrict__ rs, const double* __restrict__ y_last, double* __restrict__ part,
-           const HState* st, int phase) {
+k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const T* __restrict__ yprev,
+           const double* __restrict__ rl_s, const double* __restrict__ ru_s, const double* __restrict__ rl_o,
+           const double* __restrict__ ru_o, const double* __restrict__ rs, const double* __restrict__ y_last,
+           double* __restrict__ part, const HState* st, int phase) {
     if (st->stop || st->phase != phase) return;
     __shared__ double red[kQ * 32];
-    double v[kQ] = {0, 0, 0, 0, 0, 0};
+    double v[kQ] = {0, 0, 0, 0, 0, 0, 0};   // rp_o^2, rp_s^2, dobj, dy^2 (restart), dy^2 (step), -, nan
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const double a = ax[i];
         const double ys = static_cast<double>(yc[i]);
-        if (!isfinite(a) || !isfinite(ys)) v[5] = 1.0;
+        if (!isfinite(a) || !isfinite(ys)) v[kQ - 1] = 1.0;
+        const double fy = ys - static_cast<double>(yprev[i]);
+        v[4] += fy * fy;
         const double ps = a - fmin(fmax(a, rl_s[i]), ru_s[i]);
         const double ao = a / rs[i];
         const double po = ao - fmin(fmax(ao, rl_o[i]), ru_o[i]);
@@ -141,7 +145,7 @@ k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const
         v[3] += dy * dy;
     }
     block_reduce<OpSum, double, kQ - 1>(*reinterpret_cast<double(*)[kQ - 1]>(v), red);
-    double f[1] = {v[5]};
+    double f[1] = {v[kQ - 1]};
     block_reduce<OpMax, double, 1>(f, red);
     if (threadIdx.x == 0) {
         for (int q = 0; q < kQ - 1; ++q) part[blockIdx.x * kQ + q] = v[q];
@@ -154,16 +158,19 @@ k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const
 // objective, distance of x+ from the last restart point.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_kkt_cols(int n, const double* __restrict__ aty, const T* __restrict__ xc, const double* __restrict__ c_s,
-           const double* __restrict__ cl_o, const double* __restrict__ cu_o, const double* __restrict__ cs,
-           const double* __restrict__ x_last, double* __restrict__ part, const HState* st, int phase) {
+k_kkt_cols(int n, const double* __restrict__ aty, const T* __restrict__ xc, const T* __restrict__ xprev,
+           const double* __restrict__ c_s, const double* __restrict__ cl_o, const double* __restrict__ cu_o,
+           const double* __restrict__ cs, const double* __restrict__ x_last, double* __restrict__ part,
+           const HState* st, int phase) {
     if (st->stop || st->phase != phase) return;
     __shared__ double red[kQ * 32];
-    double v[kQ] = {0, 0, 0, 0, 0, 0};   // rd_o^2, rd_s^2, pobj, dobj, dx^2, nan
+    double v[kQ] = {0, 0, 0, 0, 0, 0, 0};   // rd_o^2, rd_s^2, pobj, dobj, dx^2 (restart), dx^2 (step), nan
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const double at = aty[j];
         const double xs = static_cast<double>(xc[j]);
-        if (!isfinite(at) || !isfinite(xs)) v[5] = 1.0;
+        if (!isfinite(at) || !isfinite(xs)) v[kQ - 1] = 1.0;
+        const double fx = xs - static_cast<double>(xprev[j]);
+        v[5] += fx * fx;
         const bool lf = finite_lo(cl_o[j]), uf = finite_up(cu_o[j]);
         const double r_s = c_s[j] + at;
         const double r_o = r_s / cs[j];
@@ -181,7 +188,7 @@ k_kkt_cols(int n, const double* __restrict__ aty, const T* __restrict__ xc, cons
         v[4] += dx * dx;
     }
     block_reduce<OpSum, double, kQ - 1>(*reinterpret_cast<double(*)[kQ - 1]>(v), red);
-    double f[1] = {v[5]};
+    double f[1] = {v[kQ - 1]};
     block_reduce<OpMax, double, 1>(f, red);
     if (threadIdx.x == 0) {
         for (int q = 0; q < kQ - 1; ++q) part[blockIdx.x * kQ + q] = v[q];
@@ -200,25 +207,30 @@ struct ControlParams {
     int phase;
     int mixed;        // 1 when an FP32 phase hands over to FP64
     int stall_checks; // FP32 stall window in checks (0 = no stall test; at most kHist - 1)
+    int metric;       // restart metric: 0 weighted KKT, 1 fixed-point residual
 };
+
+constexpr int kS = 2 * (kQ - 1);   // sums the control CTA combines (rows, then columns)
 
 __global__ void __launch_bounds__(1024)
 k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ part_c, ControlParams cp,
                   HState* st) {
     if (st->stop || st->phase != cp.phase) return;
-    __shared__ double red[10 * 32];
-    double s[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    __shared__ double red[kS * 32];
+    double s[kS];
+#pragma unroll
+    for (int q = 0; q < kS; ++q) s[q] = 0.0;
     for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x) {
-        for (int q = 0; q < kQ - 1; ++q) { s[q] += part_r[b * kQ + q]; s[5 + q] += part_c[b * kQ + q]; }
+        for (int q = 0; q < kQ - 1; ++q) { s[q] += part_r[b * kQ + q]; s[kQ - 1 + q] += part_c[b * kQ + q]; }
     }
-    block_reduce<OpSum, double, 10>(s, red);
+    block_reduce<OpSum, double, kS>(s, red);
     double f[1] = {0.0};
     for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x)
         f[0] = fmax(f[0], fmax(part_r[b * kQ + kQ - 1], part_c[b * kQ + kQ - 1]));
     block_reduce<OpMax, double, 1>(f, red);
     if (threadIdx.x != 0) return;
-    const double rp_o2 = s[0], rp_s2 = s[1], dobj_r = s[2], dy2 = s[3];
-    const double rd_o2 = s[5], rd_s2 = s[6], pobj_s = s[7], dobj_c = s[8], dx2 = s[9];
+    const double rp_o2 = s[0], rp_s2 = s[1], dobj_r = s[2], dy2 = s[3], fy2 = s[4];
+    const double rd_o2 = s[6], rd_s2 = s[7], pobj_s = s[8], dobj_c = s[9], dx2 = s[10], fx2 = s[11];
     st->total += cp.len;
     st->phase_iters[cp.phase] += cp.len;
     st->restart_flag = 0;
@@ -244,7 +256,8 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
         return;
     }
     const double omega = st->omega;
-    const double wk = sqrt(omega * rp_s2 + rd_s2 / omega + rel_gap * rel_gap);
+    const double wk = cp.metric == 1 ? sqrt(omega * fx2 + fy2 / omega)
+                                     : sqrt(omega * rp_s2 + rd_s2 / omega + rel_gap * rel_gap);
     if (cp.mixed && cp.phase == 0) {
         const int hn = st->hist_n;
         const int w = cp.stall_checks;
@@ -386,7 +399,7 @@ __global__ void k_reduced_costs(int n, const double* __restrict__ c, int is_max,
 template <typename T>
 struct Phase {
     int m = 0, n = 0, phase = 0;
-    DeviceBuffer<T> x, x0, xb, xc, y, y0, yc;
+    DeviceBuffer<T> x, x0, xb, xc, xprev, y, y0, yc, yprev;
     DeviceBuffer<T> c, cl, cu, rl, ru;          // iteration copies in T (FP64: separate copies too)
     const T* csr_val = nullptr;
     const T* csc_val = nullptr;
@@ -404,8 +417,8 @@ struct Phase {
     vajra_status alloc(int m_, int n_, const Prepared& p, cudaStream_t st) {
         m = m_; n = n_;
         for (auto& e : ev) VJ_CUDA(cudaEventCreate(&e));
-        for (auto* b : {&x, &x0, &xb, &xc, &c, &cl, &cu}) VJ_TRY(b->alloc(n));
-        for (auto* b : {&y, &y0, &yc, &rl, &ru}) VJ_TRY(b->alloc(m));
+        for (auto* b : {&x, &x0, &xb, &xc, &xprev, &c, &cl, &cu}) VJ_TRY(b->alloc(n));
+        for (auto* b : {&y, &y0, &yc, &yprev, &rl, &ru}) VJ_TRY(b->alloc(m));
         const unsigned gn = grid_for(n, kThreads, 148 * 32), gm = grid_for(m, kThreads, 148 * 32);
         k_to_t<T><<<gn, kThreads, 0, st>>>(n, p.c.get(), c.get());
         k_to_t<T><<<gn, kThreads, 0, st>>>(n, p.col_lower.get(), cl.get());
@@ -425,10 +438,10 @@ void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState
     if (timed) cudaEventRecordWithFlags(ph.ev[0], st, cudaEventRecordExternal);
     launch_spmv_t<T, T, T>(at, ph.csc_val, ph.y.get(),
                            EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                         ph.xc.get(), S, gamma, kk, ph.phase, write_cand}, st);
+                                         ph.xc.get(), ph.xprev.get(), S, gamma, kk, ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[1], st, cudaEventRecordExternal);
     launch_spmv_t<T, T, T>(a, ph.csr_val, ph.xb.get(),
-                           EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), S, gamma, kk,
+                           EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, gamma, kk,
                                        ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[2], st, cudaEventRecordExternal);
 }
@@ -442,10 +455,10 @@ void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const 
                    CheckBuffers& cb, HState* S, const ControlParams& cp, cudaStream_t st) {
     launch_spmv_t<double, T, double>(a64, p.csr_val.get(), ph.xc.get(), EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
     launch_spmv_t<double, T, double>(at64, p.csc_val.get(), ph.yc.get(), EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
-    k_kkt_rows<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.m, cb.ax.get(), ph.yc.get(), p.row_lower.get(), p.row_upper.get(),
+    k_kkt_rows<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.m, cb.ax.get(), ph.yc.get(), ph.yprev.get(), p.row_lower.get(), p.row_upper.get(),
                                                      lp.row_lower.get(), lp.row_upper.get(), p.row_scale.get(),
                                                      cb.y_last.get(), cb.part_r.get(), S, ph.phase);
-    k_kkt_cols<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.n, cb.aty.get(), ph.xc.get(), p.c.get(), lp.col_lower.get(),
+    k_kkt_cols<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.n, cb.aty.get(), ph.xc.get(), ph.xprev.get(), p.c.get(), lp.col_lower.get(),
                                                      lp.col_upper.get(), p.col_scale.get(), cb.x_last.get(),
                                                      cb.part_c.get(), S, ph.phase);
     k_halpern_control<<<1, 1024, 0, st>>>(cb.part_r.get(), cb.part_c.get(), cp, S);
@@ -565,26 +578,32 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(cb.y_last.alloc(m));
 
     // Launch shapes: FP64 views for the checks, autotuned views for the iteration precision.
+    // Launch shapes, tuned per precision: (a32, at32) for the FP32 phase, (a64, at64) for the
+    // FP64 iterations and for every FP64 check.  A handle keeps its first tuning.
     CsrView a64 = p.a, at64 = p.at;
-    CsrView a_it = p.a, at_it = p.at;
-    if (o.autotune && h->tuned_group_a > 0) {
-        a_it.group = h->tuned_group_a;
-        at_it.group = h->tuned_group_at;
-        a64.group = a_it.group;
-        at64.group = at_it.group;
-    } else if (o.autotune) {
-        if (mixed) {
-            VJ_TRY(autotune<float>(a_it, p.csr_val32.get(), p32.xb.get(), p32.yc.get(), st));
-            VJ_TRY(autotune<float>(at_it, p.csc_val32.get(), p32.y.get(), p32.xc.get(), st));
-        } else {
-            VJ_TRY(autotune<double>(a_it, p.csr_val.get(), p64.xb.get(), p64.yc.get(), st));
-            VJ_TRY(autotune<double>(at_it, p.csc_val.get(), p64.y.get(), p64.xc.get(), st));
+    CsrView a32 = p.a, at32 = p.at;
+    if (o.autotune) {
+        if (mixed && !(h->tuned & 1)) {
+            VJ_TRY(autotune<float>(a32, p.csr_val32.get(), p32.xb.get(), p32.yc.get(), st));
+            VJ_TRY(autotune<float>(at32, p.csc_val32.get(), p32.y.get(), p32.xc.get(), st));
+            h->tuned_a32 = a32.group;
+            h->tuned_at32 = at32.group;
+            h->tuned |= 1;
         }
-        a64.group = a_it.group;
-        at64.group = at_it.group;
-        h->tuned_group_a = a_it.group;
-        h->tuned_group_at = at_it.group;
+        if (!(h->tuned & 2)) {
+            VJ_TRY(autotune<double>(a64, p.csr_val.get(), p64.xb.get(), p64.yc.get(), st));
+            VJ_TRY(autotune<double>(at64, p.csc_val.get(), p64.y.get(), p64.xc.get(), st));
+            h->tuned_a64 = a64.group;
+            h->tuned_at64 = at64.group;
+            h->tuned |= 2;
+        }
+        a32.group = h->tuned_a32;
+        at32.group = h->tuned_at32;
+        a64.group = h->tuned_a64;
+        at64.group = h->tuned_at64;
     }
+    const CsrView& a_it = mixed ? a32 : a64;     // shapes reported for the dominant phase
+    const CsrView& at_it = mixed ? at32 : at64;
 
     const int mx = m > n ? m : n;
     if (mixed)
@@ -630,6 +649,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.beta_artificial = o.restart_artificial;
     cp.pw_smoothing = o.primal_weight_smoothing;
     cp.mixed = mixed ? 1 : 0;
+    cp.metric = o.restart_metric == 1 ? 1 : 0;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
     const double gamma = o.reflection;
     const int K = o.check_frequency > 0 ? o.check_frequency : 64;
@@ -643,11 +663,13 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         const int64_t remaining = max_iter - launched;
         const int len = static_cast<int>(remaining < K ? remaining : K);
         auto run_chunk = [&](auto& ph) -> vajra_status {
+            const CsrView& ia = ph.phase == 0 ? a32 : a64;
+            const CsrView& iat = ph.phase == 0 ? at32 : at64;
             if (len == K) {
                 if (!ph.exec) {
                     const int64_t before = launch_count();
                     VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                    enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, true, st);
+                    enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, gamma, len, cp, true, st);
                     VJ_CUDA(cudaStreamEndCapture(st, &ph.graph));
                     VJ_CUDA(cudaGraphInstantiate(&ph.exec, ph.graph, 0));
                     ph.graph_kernels = launch_count() - before;
@@ -656,7 +678,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 VJ_CUDA(cudaGraphLaunch(ph.exec, st));
                 note_launch(ph.graph_kernels);
             } else {
-                enqueue_chunk(ph, a_it, at_it, a64, at64, p, lp, cb, S, gamma, len, cp, false, st);
+                enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, gamma, len, cp, false, st);
                 VJ_LAUNCH_CHECK();
             }
             return VAJRA_OK;

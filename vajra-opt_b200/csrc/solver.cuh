@@ -21,8 +21,9 @@ struct vajra_pdhg {
     int64_t transfers = 0;
     // SpMV lane groups chosen by the first autotuned run of this handle; later runs reuse
     // them, so repeated runs of one handle sum in the same order and repeat bit for bit.
-    int tuned_group_a = 0;
-    int tuned_group_at = 0;
+    int tuned = 0;                       // bit 0: FP32 shapes tuned, bit 1: FP64 shapes tuned
+    int tuned_a32 = 8, tuned_at32 = 8;   // lane groups (0 = row-block kernel)
+    int tuned_a64 = 8, tuned_at64 = 8;
 };
 
 namespace vajra {
@@ -50,6 +51,8 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r);
 vajra_status run_halpern(vajra_pdhg* h, vajra_result* r);
 vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajra_result* results,
                        cudaStream_t st, double* device_time);
+vajra_status run_unrolled(int count, const vajra_lp* lps, const vajra_unrolled_opts& o, const double* weights,
+                          double* h_loss, double* h_x, double* h_gc, double* h_grl, double* h_gru, cudaStream_t st);
 
 // Closed forms for LPs without rows or without nonzeros (pdhg.cpp:88-127 for m = 0 / n = 0;
 // for nnz = 0 the rows decouple from the columns).  Returns true when it handled the LP.

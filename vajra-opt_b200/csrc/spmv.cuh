@@ -127,11 +127,27 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
         e = ptr[row + 1];
         if (e - s > long_len || skip_rows_impl(epi, row, row + 1, 0)) valid = false;
     }
+    // Memory-level parallelism: each lane first issues a batch of kBatch index / value loads,
+    // then the kBatch independent gathers, then the FMAs (predicated at the row end), so a
+    // lane waits for two memory round trips per kBatch elements instead of two per element.
+    constexpr int kBatch = 4;
     Acc acc = Acc(0);
     if (valid) {
-#pragma unroll 4
-        for (int64_t k = s + lane; k < e; k += G)
-            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+        for (int64_t base = s + lane; base < e; base += static_cast<int64_t>(G) * kBatch) {
+            int ii[kBatch];
+            VV vv[kBatch];
+#pragma unroll
+            for (int t = 0; t < kBatch; ++t) {
+                const int64_t k = base + static_cast<int64_t>(t) * G;
+                ii[t] = k < e ? ld_stream(idx + k) : -1;
+                vv[t] = k < e ? ld_stream(val + k) : VV(0);
+            }
+            VX xx[kBatch];
+#pragma unroll
+            for (int t = 0; t < kBatch; ++t) xx[t] = ii[t] >= 0 ? ld_cached(x + ii[t]) : VX(0);
+#pragma unroll
+            for (int t = 0; t < kBatch; ++t) acc = fma(static_cast<Acc>(vv[t]), static_cast<Acc>(xx[t]), acc);
+        }
     }
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -195,21 +211,36 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
     if (ptr[r1] - ptr[r1 - 1] > kTile) r_end = r1 - 1;
     if (r0 >= r_end || skip_rows_impl(epi, r0, r_end, 0)) return;
     const int64_t e0 = ptr[r0], e1 = ptr[r_end];
-    for (int64_t q = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x); q < e1; q += 4 * blockDim.x) {
-        int ii[4];
-        VV vv[4];
-        load4(idx + q, ii);
-        load4(val + q, vv);
-        Acc pr[4];
+    // A block stages fewer than 2 kTile entries, i.e. at most kQuads = 2 kTile / (4 kThreads)
+    // (+1 for alignment) aligned groups of four per thread.  All of a thread's index / value
+    // vector loads are issued first, then all its gathers, then the products are staged.
+    constexpr int kQuads = (2 * kTile) / (4 * kThreads) + 1;
+    const int64_t qbase = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x);
+    int ii[kQuads][4];
+    VV vv[kQuads][4];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int64_t k = q + t;
-            pr[t] = (k >= e0 && k < e1) ? static_cast<Acc>(vv[t]) * static_cast<Acc>(ld_cached(x + ii[t])) : Acc(0);
+    for (int u = 0; u < kQuads; ++u) {
+        const int64_t q = qbase + static_cast<int64_t>(u) * 4 * kThreads;
+        if (q < e1) {
+            load4(idx + q, ii[u]);
+            load4(val + q, vv[u]);
         }
+    }
+    VX xx[kQuads][4];
+#pragma unroll
+    for (int u = 0; u < kQuads; ++u) {
+        const int64_t q = qbase + static_cast<int64_t>(u) * 4 * kThreads;
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+            xx[u][t] = (q < e1 && q + t >= e0 && q + t < e1) ? ld_cached(x + ii[u][t]) : VX(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kQuads; ++u) {
+        const int64_t q = qbase + static_cast<int64_t>(u) * 4 * kThreads;
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             const int64_t k = q + t;
-            if (k >= e0 && k < e1) prod[k - e0] = pr[t];
+            if (q < e1 && k >= e0 && k < e1) prod[k - e0] = static_cast<Acc>(vv[u][t]) * static_cast<Acc>(xx[u][t]);
         }
     }
     if (threadIdx.x == 0) n_med = 0;

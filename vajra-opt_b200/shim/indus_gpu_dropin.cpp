@@ -70,6 +70,12 @@ Solution solve_pdhg_gpu(const Model& model, const Options& options) {
     sol.col_dual.assign(static_cast<size_t>(n), 0.0);
     sol.col_basis_status.assign(static_cast<size_t>(n), BasisStatus::kUnknown);
     sol.row_basis_status.assign(static_cast<size_t>(m), BasisStatus::kUnknown);
+    if (vajra_abi_version() != VAJRA_ABI_VERSION) {
+        sol.status = SolveStatus::kUnsupported;
+        sol.status_message = "libvajra_pdhg ABI " + std::to_string(vajra_abi_version()) +
+                             " does not match this build's header (" + std::to_string(VAJRA_ABI_VERSION) + ")";
+        return sol;
+    }
 
     vajra_lp lp{};
     lp.num_rows = m;

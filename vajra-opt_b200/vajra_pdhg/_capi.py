@@ -16,6 +16,8 @@ _fp = C.POINTER(C.c_float)
 _i64p = C.POINTER(C.c_int64)
 _i32p = C.POINTER(C.c_int32)
 
+ABI_VERSION = 3   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
+
 # vajra_status
 OK, ERR_INVALID_ARGUMENT, ERR_NO_DEVICE, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_WAIT_TIMEOUT, ERR_INTERNAL = range(7)
 ALGO_REFERENCE, ALGO_HALPERN = 0, 1
@@ -39,7 +41,7 @@ class VajraOpts(C.Structure):
                 ("autotune", C.c_int32), ("verbose", C.c_int32), ("mixed_stall_checks", C.c_int32),
                 ("restart_sufficient", C.c_double), ("restart_necessary", C.c_double),
                 ("restart_artificial", C.c_double), ("primal_weight_smoothing", C.c_double),
-                ("step_safety", C.c_double), ("reserved", C.c_int32 * 6)]
+                ("step_safety", C.c_double), ("restart_metric", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class VajraResult(C.Structure):
@@ -94,6 +96,10 @@ SIGNATURES = [
     ("vajra_is_cuda_available", C.c_int32, []),
     ("vajra_last_timing", None, [C.POINTER(VajraTiming)]),
     ("vajra_status_string", C.c_char_p, [C.c_int32]),
+    ("vajra_abi_version", C.c_int32, []),
+    ("vajra_default_unrolled_opts", None, [C.c_void_p]),
+    ("vajra_pdhg_unrolled", C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]),
     ("vajra_csr_spmv_f64", C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("vajra_csr_spmv_f32", C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("vajra_csc_spmv_transpose_f64", C.c_int32, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -116,6 +122,11 @@ def lib():
                 f"{LIB_PATH} is missing: build it with `make -C vajra-opt_b200/csrc` "
                 "(or __graft_entry__.build()); this package has no CPU fallback")
         handle = C.CDLL(LIB_PATH)
+        handle.vajra_abi_version.restype = C.c_int32
+        handle.vajra_abi_version.argtypes = []
+        got = handle.vajra_abi_version()
+        if got != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {got}, these bindings expect {ABI_VERSION}: rebuild")
         for name, res, args in SIGNATURES:
             fn = getattr(handle, name)
             fn.restype = res
