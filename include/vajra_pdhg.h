@@ -324,6 +324,26 @@ vajra_status vajra_pdhg_step_f64(int32_t rows, int32_t cols,
                                  double* x, double* x_bar, double* y, double* w, double* v,
                                  void* stream);
 
+/* FP64 relative KKT (the definition the solver's checks use) of a point (x, y) of an LP whose
+ * data the caller already holds on the device: A as CSR and as CSC, c, bounds, the column
+ * values x and the row duals y in the verifier's sign convention of the minimisation form.
+ * out (device, 6 doubles) = rel_primal, rel_dual, rel_gap, rel_kkt, primal and dual
+ * objective (minimisation form, offset included).
+ * No counterpart in the reference.  It allocates nothing, for callers that cannot call
+ * cudaMalloc: its scratch is a fixed 2 MiB device array inside the library, which limits
+ * rows and columns to 8,388,608 each (larger sizes return VAJRA_ERR_INVALID_ARGUMENT).  The
+ * first call on a device looks up that array's address; make it before any stream capture.
+ * Nothing has to start at zero: each call writes every partial sum it later reads.  All calls
+ * on a device share the array: calls that overlap on the GPU race. */
+vajra_status vajra_relative_kkt_noalloc_f64(int32_t rows, int32_t cols, const int64_t* row_ptr,
+                                            const int32_t* col_idx, const double* csr_values,
+                                            const int64_t* col_ptr, const int32_t* row_idx,
+                                            const double* csc_values, const double* c,
+                                            const double* col_lower, const double* col_upper,
+                                            const double* row_lower, const double* row_upper,
+                                            const double* x, const double* y, int32_t sense,
+                                            double objective_offset, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

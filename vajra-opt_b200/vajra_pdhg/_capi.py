@@ -108,6 +108,8 @@ SIGNATURES = [
     ("vajra_primal_prox_f64", C.c_int32, [C.c_int32, C.c_double] + [C.c_void_p] * 7),
     ("vajra_device_diagnostics_f64", C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 11),
     ("vajra_pdhg_step_f64", C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 11 + [C.c_double, C.c_double] + [C.c_void_p] * 6),
+    ("vajra_relative_kkt_noalloc_f64", C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 13
+     + [C.c_int32, C.c_double, C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None
