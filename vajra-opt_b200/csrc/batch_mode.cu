@@ -55,20 +55,33 @@ struct EpiBPrimal {
     BatchArrays S;
     double gamma;
     int kk, write_cand;
+    // two-phase (spmv.cuh): the instance lookups and vector loads go out before the SpMV's
+    struct Pre { double k, tau, xo, c, cl, cu, x0; int done; };
     __device__ bool active() const { return true; }
     __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, col_inst, r0, r1); }
-    __device__ void operator()(int j, double v) const {
-        const int i = col_inst[j];
-        if (S.done[i]) return;
-        const double k = static_cast<double>(S.k_base[i] + kk);
-        const double w1 = (k + 1.0) / (k + 2.0), w0 = 1.0 / (k + 2.0);
-        const double xo = x[j];
-        double xp = xo - S.tau[i] * (c[j] + v);
-        xp = xp < cl[j] ? cl[j] : (xp > cu[j] ? cu[j] : xp);
-        xb[j] = xp + xp - xo;
-        x[j] = w1 * ((1.0 + gamma) * xp - gamma * xo) + w0 * x0[j];
+    __device__ Pre pre(int j) const {
+        const int i = __ldg(col_inst + j);
+        Pre p;
+        p.done = S.done[i];
+        p.k = static_cast<double>(S.k_base[i] + kk);
+        p.tau = S.tau[i];
+        p.xo = x[j];
+        p.c = __ldg(c + j);
+        p.cl = __ldg(cl + j);
+        p.cu = __ldg(cu + j);
+        p.x0 = __ldg(x0 + j);
+        return p;
+    }
+    __device__ void operator()(int j, double v, const Pre& p) const {
+        if (p.done) return;
+        const double w1 = (p.k + 1.0) / (p.k + 2.0), w0 = 1.0 / (p.k + 2.0);
+        double xp = p.xo - p.tau * (p.c + v);
+        xp = xp < p.cl ? p.cl : (xp > p.cu ? p.cu : xp);
+        xb[j] = xp + xp - p.xo;
+        x[j] = w1 * ((1.0 + gamma) * xp - gamma * p.xo) + w0 * p.x0;
         if (write_cand) xc[j] = xp;
     }
+    __device__ void operator()(int j, double v) const { (*this)(j, v, pre(j)); }
 };
 
 struct EpiBDual {
@@ -78,22 +91,33 @@ struct EpiBDual {
     BatchArrays S;
     double gamma;
     int kk, write_cand;
+    struct Pre { double k, sigma, yo, rl, ru, y0; int done; };
     __device__ bool active() const { return true; }
     __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, row_inst, r0, r1); }
-    __device__ void operator()(int r, double w) const {
-        const int i = row_inst[r];
-        if (S.done[i]) return;
-        const double k = static_cast<double>(S.k_base[i] + kk);
-        const double w1 = (k + 1.0) / (k + 2.0), w0 = 1.0 / (k + 2.0);
-        const double sg = S.sigma[i];
-        const double yo = y[r];
-        const double yh = yo + sg * w;
+    __device__ Pre pre(int r) const {
+        const int i = __ldg(row_inst + r);
+        Pre p;
+        p.done = S.done[i];
+        p.k = static_cast<double>(S.k_base[i] + kk);
+        p.sigma = S.sigma[i];
+        p.yo = y[r];
+        p.rl = __ldg(rl + r);
+        p.ru = __ldg(ru + r);
+        p.y0 = __ldg(y0 + r);
+        return p;
+    }
+    __device__ void operator()(int r, double w, const Pre& p) const {
+        if (p.done) return;
+        const double w1 = (p.k + 1.0) / (p.k + 2.0), w0 = 1.0 / (p.k + 2.0);
+        const double sg = p.sigma;
+        const double yh = p.yo + sg * w;
         double q = yh / sg;
-        q = q < rl[r] ? rl[r] : (q > ru[r] ? ru[r] : q);
+        q = q < p.rl ? p.rl : (q > p.ru ? p.ru : q);
         const double yp = yh - sg * q;
-        y[r] = w1 * ((1.0 + gamma) * yp - gamma * yo) + w0 * y0[r];
+        y[r] = w1 * ((1.0 + gamma) * yp - gamma * p.yo) + w0 * p.y0;
         if (write_cand) yc[r] = yp;
     }
+    __device__ void operator()(int r, double w) const { (*this)(r, w, pre(r)); }
 };
 
 struct EpiBStore {
@@ -111,6 +135,63 @@ struct EpiStorePlain {
     double* out;
     __device__ bool active() const { return true; }
     __device__ void operator()(int r, double s) const { out[r] = s; }
+};
+
+// Blocks of one launch shape that hold at least one row of an unfinished instance (order
+// irrelevant: every row's result is independent of which CTA computes it).
+__global__ void k_active_blocks(int nblocks, int rows, int rows_per_block, const int32_t* __restrict__ block_rows,
+                                const int* __restrict__ inst, const int* __restrict__ done,
+                                int32_t* __restrict__ list, int* __restrict__ count) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    int r0, r1;
+    if (block_rows) {
+        r0 = block_rows[b];
+        r1 = block_rows[b + 1];
+    } else {
+        r0 = b * rows_per_block;
+        r1 = r0 + rows_per_block < rows ? r0 + rows_per_block : rows;
+    }
+    if (r0 < r1 && any_active(done, inst, r0, r1)) list[atomicAdd(count, 1)] = b;
+}
+
+// The active-block list of one iteration view (list mode of spmv.cuh).
+struct BlockList {
+    DeviceBuffer<int32_t> list;
+    DeviceBuffer<int> count;
+    int nblocks = 0, rows = 0, rows_per_block = 0;
+    const int32_t* block_rows = nullptr;
+    const int* inst = nullptr;
+    // Builds the shape description for `v` (as tuned) and switches `v` to list mode.
+    vajra_status attach(CsrView& v, const int* inst_, int sms) {
+        inst = inst_;
+        rows = v.rows;
+        int cap;
+        if (v.group == 0 && v.block_rows) {
+            nblocks = v.nb;
+            block_rows = v.block_rows;
+            cap = sms * 4;
+        } else {
+            int g = v.group;
+            if (g != 1 && g != 2 && g != 4 && g != 8 && g != 16) g = g == 0 ? 8 : 32;   // launch_spmv_t's dispatch
+            rows_per_block = kThreads / g;
+            nblocks = vec_block_count(v.rows, g);
+            cap = sms * 8;
+        }
+        VJ_TRY(list.alloc(static_cast<size_t>(nblocks > 0 ? nblocks : 1)));
+        VJ_TRY(count.alloc(1));
+        v.blk_list = list.get();
+        v.blk_count = count.get();
+        v.blk_grid = nblocks < cap ? (nblocks > 0 ? nblocks : 1) : cap;
+        return VAJRA_OK;
+    }
+    void rebuild(const int* done, cudaStream_t st) {
+        cudaMemsetAsync(count.get(), 0, sizeof(int), st);
+        if (nblocks > 0)
+            k_active_blocks<<<grid_for(nblocks), kThreads, 0, st>>>(nblocks, rows, rows_per_block, block_rows, inst, done,
+                                                                   list.get(), count.get());
+        note_launch(1);
+    }
 };
 
 __device__ __forceinline__ bool lo_fin(double l) { return l > -1e20; }
@@ -524,6 +605,19 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
         cudaEventDestroy(e1);
     }
 
+    // Iteration views in list mode: only blocks of unfinished instances run (rebuilt at the
+    // start of every chunk, after the previous check decided which instances are done).
+    int sms = 148;
+    {
+        int dev = 0;
+        VJ_CUDA(cudaGetDevice(&dev));
+        VJ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    CsrView a_it = a, at_it = at;
+    BlockList list_a, list_at;
+    VJ_TRY(list_a.attach(a_it, row_inst.get(), sms));
+    VJ_TRY(list_at.attach(at_it, col_inst.get(), sms));
+
     DeviceBuffer<BatchCounters> counters;
     VJ_TRY(counters.alloc(1));
     BatchCounters* hc = nullptr;
@@ -545,19 +639,21 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     int64_t graph_kernels = 0;
 
     auto enqueue_chunk = [&](int len) {
+        list_a.rebuild(S.done, st);
+        list_at.rebuild(S.done, st);
         for (int kk = 0; kk < len; ++kk) {
             const int wc = kk == len - 1 ? 1 : 0;
             launch_spmv_t<double, double, double>(
-                at, p.csc_val.get(), y.get(),
+                at_it, p.csc_val.get(), y.get(),
                 EpiBPrimal{p.c.get(), p.col_lower.get(), p.col_upper.get(), x0.get(), x.get(), xb.get(), xc.get(),
                            col_inst.get(), S, gamma, kk, wc}, st);
             launch_spmv_t<double, double, double>(
-                a, p.csr_val.get(), xb.get(),
+                a_it, p.csr_val.get(), xb.get(),
                 EpiBDual{p.row_lower.get(), p.row_upper.get(), y0.get(), y.get(), yc.get(), row_inst.get(), S, gamma,
                          kk, wc}, st);
         }
-        launch_spmv_t<double, double, double>(a, p.csr_val.get(), xc.get(), EpiBStore{ax.get(), row_inst.get(), S.done}, st);
-        launch_spmv_t<double, double, double>(at, p.csc_val.get(), yc.get(), EpiBStore{aty.get(), col_inst.get(), S.done}, st);
+        launch_spmv_t<double, double, double>(a_it, p.csr_val.get(), xc.get(), EpiBStore{ax.get(), row_inst.get(), S.done}, st);
+        launch_spmv_t<double, double, double>(at_it, p.csc_val.get(), yc.get(), EpiBStore{aty.get(), col_inst.get(), S.done}, st);
         k_bkkt<<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), ax.get(), aty.get(), xc.get(), yc.get(),
                                            p.row_lower.get(), p.row_upper.get(), lp.row_lower.get(), lp.row_upper.get(),
                                            p.row_scale.get(), p.c.get(), lp.col_lower.get(), lp.col_upper.get(),

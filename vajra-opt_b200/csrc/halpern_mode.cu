@@ -18,6 +18,7 @@
 #include <cstring>
 #include <vector>
 
+#include "halpern_state.cuh"
 #include "solver.cuh"
 
 namespace vajra {
@@ -25,91 +26,6 @@ namespace {
 
 constexpr int kQ = 7;             // partial sums per block in the check passes (last: NaN flag)
 constexpr int kCheckBlocks = 148 * 4;
-constexpr int kHist = 16;
-
-struct HState {
-    double omega, eta, tau, sigma;
-    double kkt_start, kkt_prev;
-    double rel_p, rel_d, rel_gap, rel_kkt, pobj, dobj;
-    double bnorm, cnorm, offset_min;
-    double hist[kHist];
-    long long k_base;
-    long long total;
-    long long phase_iters[2];
-    long long stop_iter;
-    int hist_n;
-    int phase;          // 0: FP32 phase of the mixed mode, 1: FP64
-    int stop;
-    int status;
-    int restart_count;
-    int restart_flag;
-    int switch_flag;
-    int pad;
-};
-
-constexpr int kStatusOptimal = 1;
-constexpr int kStatusIterLimit = 6;
-constexpr int kStatusTimeLimit = 7;
-constexpr int kStatusNumerical = 9;
-
-// At the last iteration of a chunk (write_cand) the epilogues also keep T(z) (xc, yc) and
-// the point it was taken from (xprev, yprev) for the check.
-template <typename T>
-struct EpiHPrimal {
-    const T* c; const T* cl; const T* cu; const T* x0;
-    T* x; T* xb; T* xc; T* xprev;
-    const HState* st;
-    double gamma;
-    int kk, phase, write_cand;
-    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
-    template <typename Acc>
-    __device__ void operator()(int j, Acc v) const {
-        const double k = static_cast<double>(st->k_base + kk);
-        const T w1 = static_cast<T>((k + 1.0) / (k + 2.0));
-        const T w0 = static_cast<T>(1.0 / (k + 2.0));
-        const T tau = static_cast<T>(st->tau);
-        const T g = static_cast<T>(gamma);
-        const T xo = x[j];
-        T xp = xo - tau * (c[j] + static_cast<T>(v));
-        xp = xp < cl[j] ? cl[j] : (xp > cu[j] ? cu[j] : xp);
-        xb[j] = xp + xp - xo;
-        x[j] = w1 * ((T(1) + g) * xp - g * xo) + w0 * x0[j];
-        if (write_cand) { xc[j] = xp; xprev[j] = xo; }
-    }
-};
-
-template <typename T>
-struct EpiHDual {
-    const T* rl; const T* ru; const T* y0;
-    T* y; T* yc; T* yprev;
-    const HState* st;
-    double gamma;
-    int kk, phase, write_cand;
-    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
-    template <typename Acc>
-    __device__ void operator()(int i, Acc w) const {
-        const double k = static_cast<double>(st->k_base + kk);
-        const T w1 = static_cast<T>((k + 1.0) / (k + 2.0));
-        const T w0 = static_cast<T>(1.0 / (k + 2.0));
-        const T sigma = static_cast<T>(st->sigma);
-        const T g = static_cast<T>(gamma);
-        const T yo = y[i];
-        const T yh = yo + sigma * static_cast<T>(w);
-        T q = yh / sigma;
-        q = q < rl[i] ? rl[i] : (q > ru[i] ? ru[i] : q);
-        const T yp = yh - sigma * q;
-        y[i] = w1 * ((T(1) + g) * yp - g * yo) + w0 * y0[i];
-        if (write_cand) { yc[i] = yp; yprev[i] = yo; }
-    }
-};
-
-struct EpiStoreActive {
-    double* out;
-    const HState* st;
-    int phase;
-    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
-    template <typename Acc> __device__ void operator()(int i, Acc s) const { out[i] = static_cast<double>(s); }
-};
 
 __device__ __forceinline__ bool finite_lo(double l) { return l > -1e20; }
 __device__ __forceinline__ bool finite_up(double u) { return u < 1e20; }
@@ -481,31 +397,55 @@ void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrV
     enqueue_check(ph, a64, at64, p, lp, cb, S, cp, st);
 }
 
-// Times every lane-group size of one SpMV (store epilogue) and keeps the fastest.
+// Times every launch shape (row-block kernel, 1..32 lanes per row) of both iteration kernels
+// with their real epilogues and keeps the fastest per matrix.  `tune_state` is a scratch
+// state whose phase is the tuned one; the iterates it scribbles on are re-initialised after.
 template <typename T>
-vajra_status autotune(CsrView& v, const T* val, const T* xin, T* out, cudaStream_t st) {
-    if (v.rows <= 0) return VAJRA_OK;
+vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* tune_state, double gamma,
+                                cudaStream_t st) {
     cudaEvent_t e0, e1;
     VJ_CUDA(cudaEventCreate(&e0));
     VJ_CUDA(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int best_g = v.group;
-    for (int g : {0, 1, 2, 4, 8, 16, 32}) {   // 0: row-block kernel, else lanes per row
-        CsrView t = v;
-        t.group = g;
-        launch_spmv_t<T, T, T>(t, val, xin, EpiStore<T>{out}, st);     // warm
-        VJ_CUDA(cudaEventRecord(e0, st));
-        for (int r = 0; r < 3; ++r) launch_spmv_t<T, T, T>(t, val, xin, EpiStore<T>{out}, st);
-        VJ_CUDA(cudaEventRecord(e1, st));
-        VJ_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        VJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) { best = ms; best_g = g; }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    v.group = best_g;
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
+    auto time_shapes = [&](CsrView& v, auto launch) -> vajra_status {
+        if (v.rows <= 0) return VAJRA_OK;
+        float best = 1e30f;
+        int best_g = v.group;
+        for (int g : {0, 1, 2, 4, 8, 16, 32}) {
+            CsrView t = v;
+            t.group = g;
+            launch(t);   // warm
+            VJ_CUDA(cudaEventRecord(e0, st));
+            for (int r = 0; r < 3; ++r) launch(t);
+            VJ_CUDA(cudaEventRecord(e1, st));
+            VJ_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            VJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) { best = ms; best_g = g; }
+        }
+        v.group = best_g;
+        return VAJRA_OK;
+    };
+    VJ_TRY(time_shapes(at, [&](const CsrView& t) {
+        launch_spmv_t<T, T, T>(t, ph.csc_val, ph.y.get(),
+                               EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
+                                             ph.xc.get(), ph.xprev.get(), tune_state, gamma, 0, ph.phase, 0}, st);
+    }));
+    VJ_TRY(time_shapes(a, [&](const CsrView& t) {
+        launch_spmv_t<T, T, T>(t, ph.csr_val, ph.xb.get(),
+                               EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
+                                           tune_state, gamma, 0, ph.phase, 0}, st);
+    }));
     return VAJRA_OK;
+}
+
+template <typename T>
+void init_iterates(Phase<T>& ph, const Prepared& p, CheckBuffers& cb, cudaStream_t st) {
+    const int mx = ph.m > ph.n ? ph.m : ph.n;
+    k_init_iterates<T><<<grid_for(mx), kThreads, 0, st>>>(ph.m, ph.n, p.col_lower.get(), p.col_upper.get(), ph.x.get(),
+                                                          ph.x0.get(), ph.xb.get(), ph.xc.get(), ph.y.get(), ph.y0.get(),
+                                                          ph.yc.get(), cb.x_last.get(), cb.y_last.get());
+    note_launch(1);
 }
 
 }  // namespace
@@ -577,46 +517,6 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(cb.x_last.alloc(n));
     VJ_TRY(cb.y_last.alloc(m));
 
-    // Launch shapes: FP64 views for the checks, autotuned views for the iteration precision.
-    // Launch shapes, tuned per precision: (a32, at32) for the FP32 phase, (a64, at64) for the
-    // FP64 iterations and for every FP64 check.  A handle keeps its first tuning.
-    CsrView a64 = p.a, at64 = p.at;
-    CsrView a32 = p.a, at32 = p.at;
-    if (o.autotune) {
-        if (mixed && !(h->tuned & 1)) {
-            VJ_TRY(autotune<float>(a32, p.csr_val32.get(), p32.xb.get(), p32.yc.get(), st));
-            VJ_TRY(autotune<float>(at32, p.csc_val32.get(), p32.y.get(), p32.xc.get(), st));
-            h->tuned_a32 = a32.group;
-            h->tuned_at32 = at32.group;
-            h->tuned |= 1;
-        }
-        if (!(h->tuned & 2)) {
-            VJ_TRY(autotune<double>(a64, p.csr_val.get(), p64.xb.get(), p64.yc.get(), st));
-            VJ_TRY(autotune<double>(at64, p.csc_val.get(), p64.y.get(), p64.xc.get(), st));
-            h->tuned_a64 = a64.group;
-            h->tuned_at64 = at64.group;
-            h->tuned |= 2;
-        }
-        a32.group = h->tuned_a32;
-        at32.group = h->tuned_at32;
-        a64.group = h->tuned_a64;
-        at64.group = h->tuned_at64;
-    }
-    const CsrView& a_it = mixed ? a32 : a64;     // shapes reported for the dominant phase
-    const CsrView& at_it = mixed ? at32 : at64;
-
-    const int mx = m > n ? m : n;
-    if (mixed)
-        k_init_iterates<float><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), p32.x.get(),
-                                                                 p32.x0.get(), p32.xb.get(), p32.xc.get(), p32.y.get(),
-                                                                 p32.y0.get(), p32.yc.get(), cb.x_last.get(), cb.y_last.get());
-    else
-        k_init_iterates<double><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), p64.x.get(),
-                                                                  p64.x0.get(), p64.xb.get(), p64.xc.get(), p64.y.get(),
-                                                                  p64.y0.get(), p64.yc.get(), cb.x_last.get(), cb.y_last.get());
-    VJ_LAUNCH_CHECK();
-    note_launch(1);
-
     HState init{};
     const double eta = (o.step_safety > 0.0 && o.step_safety < 1.0 ? o.step_safety : 0.99) / spectral_norm;
     init.omega = (hn[2] > 1e-10 && hn[3] > 1e-10) ? hn[3] / hn[2] : 1.0;
@@ -632,6 +532,47 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     init.rel_kkt = 1e30;
     DeviceBuffer<HState> dstate;
     VJ_TRY(dstate.alloc(1));
+
+    // Launch shapes, tuned per precision with the real iteration kernels: (a32, at32) for the
+    // FP32 phase, (a64, at64) for the FP64 iterations; every FP64 check uses (a64, at64) too.
+    // A handle keeps its first tuning.
+    const double gamma = o.reflection;
+    CsrView a64 = p.a, at64 = p.at;
+    CsrView a32 = p.a, at32 = p.at;
+    if (o.autotune && (!(h->tuned & 2) || (mixed && !(h->tuned & 1)))) {
+        HState tune = init;
+        if (mixed && !(h->tuned & 1)) {
+            tune.phase = 0;
+            VJ_CUDA(cudaMemcpyAsync(dstate.get(), &tune, sizeof(tune), cudaMemcpyHostToDevice, st));
+            init_iterates(p32, p, cb, st);
+            VJ_TRY(autotune_iteration<float>(p32, a32, at32, dstate.get(), gamma, st));
+            h->tuned_a32 = a32.group;
+            h->tuned_at32 = at32.group;
+            h->tuned |= 1;
+        }
+        if (!(h->tuned & 2)) {
+            tune.phase = 1;
+            VJ_CUDA(cudaMemcpyAsync(dstate.get(), &tune, sizeof(tune), cudaMemcpyHostToDevice, st));
+            init_iterates(p64, p, cb, st);
+            VJ_TRY(autotune_iteration<double>(p64, a64, at64, dstate.get(), gamma, st));
+            h->tuned_a64 = a64.group;
+            h->tuned_at64 = at64.group;
+            h->tuned |= 2;
+        }
+    }
+    if (o.autotune) {
+        a32.group = h->tuned_a32;
+        at32.group = h->tuned_at32;
+        a64.group = h->tuned_a64;
+        at64.group = h->tuned_at64;
+    }
+    const CsrView& a_it = mixed ? a32 : a64;     // shapes reported for the dominant phase
+    const CsrView& at_it = mixed ? at32 : at64;
+
+    const int mx = m > n ? m : n;
+    if (mixed) init_iterates(p32, p, cb, st);
+    else init_iterates(p64, p, cb, st);
+    VJ_LAUNCH_CHECK();
     VJ_CUDA(cudaMemcpyAsync(dstate.get(), &init, sizeof(init), cudaMemcpyHostToDevice, st));
     VJ_CUDA(cudaStreamSynchronize(st));
     const double setup_time = seconds_since(t_start);
@@ -651,7 +592,6 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.mixed = mixed ? 1 : 0;
     cp.metric = o.restart_metric == 1 ? 1 : 0;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
-    const double gamma = o.reflection;
     const int K = o.check_frequency > 0 ? o.check_frequency : 64;
     const int64_t max_iter = o.iteration_limit;
 

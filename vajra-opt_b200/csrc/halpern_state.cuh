@@ -1,0 +1,119 @@
+// Device state of VAJRA_ALGO_HALPERN and the epilogues its two iteration kernels fuse into
+// the SpMVs (x+ / x_bar / Halpern for the primal half, y+ / Halpern for the dual half).
+#pragma once
+
+#include "common.cuh"
+
+namespace vajra {
+
+constexpr int kHist = 16;
+
+struct HState {
+    double omega, eta, tau, sigma;
+    double kkt_start, kkt_prev;
+    double rel_p, rel_d, rel_gap, rel_kkt, pobj, dobj;
+    double bnorm, cnorm, offset_min;
+    double hist[kHist];
+    long long k_base;
+    long long total;
+    long long phase_iters[2];
+    long long stop_iter;
+    int hist_n;
+    int phase;          // 0: FP32 phase of the mixed mode, 1: FP64
+    int stop;
+    int status;
+    int restart_count;
+    int restart_flag;
+    int switch_flag;
+    int pad;
+};
+
+constexpr int kStatusOptimal = 1;
+constexpr int kStatusIterLimit = 6;
+constexpr int kStatusTimeLimit = 7;
+constexpr int kStatusNumerical = 9;
+
+// At the last iteration of a chunk (write_cand) the epilogues also keep T(z) (xc, yc) and
+// the point it was taken from (xprev, yprev) for the check.
+// Both epilogues are two-phase (see spmv.cuh): pre() issues every load that does not need
+// the row sum -- the read-only vectors and the device scalars through the read-only path
+// (they are written only by other kernels) -- before the SpMV's own loads.
+template <typename T>
+struct EpiHPrimal {
+    const T* c; const T* cl; const T* cu; const T* x0;
+    T* x; T* xb; T* xc; T* xprev;
+    const HState* st;
+    double gamma;
+    int kk, phase, write_cand;
+    struct Pre { T xo, c, cl, cu, x0, tau; double k; };
+    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
+    __device__ Pre pre(int j) const {
+        Pre p;
+        p.k = static_cast<double>(__ldg(&st->k_base) + kk);
+        p.tau = static_cast<T>(__ldg(&st->tau));
+        p.xo = x[j];
+        p.c = __ldg(c + j);
+        p.cl = __ldg(cl + j);
+        p.cu = __ldg(cu + j);
+        p.x0 = __ldg(x0 + j);
+        return p;
+    }
+    template <typename Acc>
+    __device__ void operator()(int j, Acc v, const Pre& p) const {
+        const T w1 = static_cast<T>((p.k + 1.0) / (p.k + 2.0));
+        const T w0 = static_cast<T>(1.0 / (p.k + 2.0));
+        const T g = static_cast<T>(gamma);
+        T xp = p.xo - p.tau * (p.c + static_cast<T>(v));
+        xp = xp < p.cl ? p.cl : (xp > p.cu ? p.cu : xp);
+        xb[j] = xp + xp - p.xo;
+        x[j] = w1 * ((T(1) + g) * xp - g * p.xo) + w0 * p.x0;
+        if (write_cand) { xc[j] = xp; xprev[j] = p.xo; }
+    }
+    template <typename Acc>
+    __device__ void operator()(int j, Acc v) const { (*this)(j, v, pre(j)); }
+};
+
+template <typename T>
+struct EpiHDual {
+    const T* rl; const T* ru; const T* y0;
+    T* y; T* yc; T* yprev;
+    const HState* st;
+    double gamma;
+    int kk, phase, write_cand;
+    struct Pre { T yo, rl, ru, y0, sigma; double k; };
+    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
+    __device__ Pre pre(int i) const {
+        Pre p;
+        p.k = static_cast<double>(__ldg(&st->k_base) + kk);
+        p.sigma = static_cast<T>(__ldg(&st->sigma));
+        p.yo = y[i];
+        p.rl = __ldg(rl + i);
+        p.ru = __ldg(ru + i);
+        p.y0 = __ldg(y0 + i);
+        return p;
+    }
+    template <typename Acc>
+    __device__ void operator()(int i, Acc w, const Pre& p) const {
+        const T w1 = static_cast<T>((p.k + 1.0) / (p.k + 2.0));
+        const T w0 = static_cast<T>(1.0 / (p.k + 2.0));
+        const T g = static_cast<T>(gamma);
+        const T yh = p.yo + p.sigma * static_cast<T>(w);
+        T q = yh / p.sigma;
+        q = q < p.rl ? p.rl : (q > p.ru ? p.ru : q);
+        const T yp = yh - p.sigma * q;
+        y[i] = w1 * ((T(1) + g) * yp - g * p.yo) + w0 * p.y0;
+        if (write_cand) { yc[i] = yp; yprev[i] = p.yo; }
+    }
+    template <typename Acc>
+    __device__ void operator()(int i, Acc w) const { (*this)(i, w, pre(i)); }
+};
+
+struct EpiStoreActive {
+    double* out;
+    const HState* st;
+    int phase;
+    __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
+    template <typename Acc> __device__ void operator()(int i, Acc s) const { out[i] = static_cast<double>(s); }
+};
+
+}  // namespace vajra

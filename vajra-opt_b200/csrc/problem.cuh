@@ -42,6 +42,7 @@ struct Prepared {
     DeviceBuffer<int32_t> long_rows_a, long_rows_at;
     // row-block partitions (block boundaries) and their rows longer than kTile
     DeviceBuffer<int32_t> rb_blocks_a, rb_blocks_at, rb_long_a, rb_long_at;
+    DeviceBuffer<TileDesc> rb_tiles_a, rb_tiles_at;
     bool scaled = false;
     CsrView a, at;                            // A (rows = m) and A^T (rows = n)
 };
@@ -58,6 +59,8 @@ struct SetupState {
     double spectral_norm;
     int power_iter;
     int pad;
+    unsigned long long row_err_bits;   // this Ruiz pass's max |1 - row norm| (bit pattern, atomicMax)
+    unsigned long long col_err_bits;
 };
 
 vajra_status upload_lp(const vajra_lp* lp, DeviceLp& d, cudaStream_t st);

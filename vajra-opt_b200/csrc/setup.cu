@@ -116,48 +116,58 @@ vajra_status build_csr(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
 // ---------------------------------------------------------------------------------------
 // scaling (Ruiz: src/linalg/scaling.cpp:7-153, in its evaluation order)
 // ---------------------------------------------------------------------------------------
+// The per-row / per-column l-inf norms, plus each block's max |1 - norm| over norms > 1e-11
+// folded into the pass-wide maximum with one atomicMax per block on the bit pattern (for
+// non-negative doubles the bit order is the value order, so the result is the exact maximum
+// whatever the block order).
 __global__ void k_col_inf(int n, const int64_t* __restrict__ col_ptr, const double* __restrict__ v,
-                          double* __restrict__ col_inf, const SetupState* sst) {
+                          double* __restrict__ col_inf, SetupState* sst) {
     if (sst->ruiz_done) return;
+    __shared__ double red[32];
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    double mx = 0.0;
-    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
-        const double a = fabs(v[k]);
-        if (a > mx) mx = a;
+    double e[1] = {0.0};
+    if (j < n) {
+        double mx = 0.0;
+        for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) {
+            const double a = fabs(v[k]);
+            if (a > mx) mx = a;
+        }
+        col_inf[j] = mx;
+        if (mx > kZeroDrop) e[0] = fabs(1.0 - mx);
     }
-    col_inf[j] = mx;
+    block_reduce<OpMax, double, 1>(e, red);
+    if (threadIdx.x == 0) atomicMax(&sst->col_err_bits, static_cast<unsigned long long>(__double_as_longlong(e[0])));
 }
 
 __global__ void k_row_inf(int m, const int64_t* __restrict__ csr_ptr, const int64_t* __restrict__ perm,
-                          const double* __restrict__ v, double* __restrict__ row_inf, const SetupState* sst) {
+                          const double* __restrict__ v, double* __restrict__ row_inf, SetupState* sst) {
     if (sst->ruiz_done) return;
+    __shared__ double red[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    double mx = 0.0;
-    for (int64_t k = csr_ptr[i]; k < csr_ptr[i + 1]; ++k) {
-        const double a = fabs(v[perm[k]]);
-        if (a > mx) mx = a;
+    double e[1] = {0.0};
+    if (i < m) {
+        double mx = 0.0;
+        for (int64_t k = csr_ptr[i]; k < csr_ptr[i + 1]; ++k) {
+            const double a = fabs(v[perm[k]]);
+            if (a > mx) mx = a;
+        }
+        row_inf[i] = mx;
+        if (mx > kZeroDrop) e[0] = fabs(1.0 - mx);
     }
-    row_inf[i] = mx;
+    block_reduce<OpMax, double, 1>(e, red);
+    if (threadIdx.x == 0) atomicMax(&sst->row_err_bits, static_cast<unsigned long long>(__double_as_longlong(e[0])));
 }
 
-// One CTA: max |1 - inf| over rows / columns with inf > 1e-11, then the convergence test.
-__global__ void k_ruiz_err(int m, int n, const double* __restrict__ row_inf, const double* __restrict__ col_inf,
-                           double tol, SetupState* sst) {
+// The Ruiz convergence test of the pass (scaling.cpp:54-70), then reset for the next pass.
+__global__ void k_ruiz_err(double tol, SetupState* sst) {
     if (sst->ruiz_done) return;
-    __shared__ double red[2 * 32];
-    double v[2] = {0.0, 0.0};
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        if (row_inf[i] > kZeroDrop) { const double e = fabs(1.0 - row_inf[i]); if (e > v[0]) v[0] = e; }
-    for (int j = threadIdx.x; j < n; j += blockDim.x)
-        if (col_inf[j] > kZeroDrop) { const double e = fabs(1.0 - col_inf[j]); if (e > v[1]) v[1] = e; }
-    block_reduce<OpMax, double, 2>(v, red);
-    if (threadIdx.x == 0) {
-        sst->ruiz_row_err = v[0];
-        sst->ruiz_col_err = v[1];
-        if (v[0] <= tol && v[1] <= tol) sst->ruiz_done = 1;
-    }
+    const double re = __longlong_as_double(static_cast<long long>(sst->row_err_bits));
+    const double ce = __longlong_as_double(static_cast<long long>(sst->col_err_bits));
+    sst->ruiz_row_err = re;
+    sst->ruiz_col_err = ce;
+    if (re <= tol && ce <= tol) sst->ruiz_done = 1;
+    sst->row_err_bits = 0ull;
+    sst->col_err_bits = 0ull;
 }
 
 // r = 1/sqrt(norm) (1 where norm <= 1e-11); cumulative scale *= r.
@@ -171,15 +181,15 @@ __global__ void k_scale_factors(int k_count, const double* __restrict__ norm, do
     scale[i] = __dmul_rn(scale[i], r);
 }
 
-// A_ij *= r_i * c_j (scaling.cpp:92-100: the product of the two factors first).
-__global__ void k_scale_matrix(int n, const int64_t* __restrict__ col_ptr, const int32_t* __restrict__ row_idx,
+// A_ij *= r_i * c_j (scaling.cpp:92-100: the product of the two factors first), one entry
+// per thread (col_of: the column of every CSC entry).
+__global__ void k_scale_matrix(int64_t nnz, const int32_t* __restrict__ col_of, const int32_t* __restrict__ row_idx,
                                double* __restrict__ v, const double* __restrict__ r, const double* __restrict__ cs,
                                const SetupState* sst, int respect_done) {
     if (respect_done && sst->ruiz_done) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const double cj = cs[j];
-    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) v[k] = __dmul_rn(v[k], __dmul_rn(r[row_idx[k]], cj));
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nnz;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        v[k] = __dmul_rn(v[k], __dmul_rn(r[row_idx[k]], cs[col_of[k]]));
 }
 
 // Pock-Chambolle (alpha = 1) norms: sum |a| per column / per row, in storage order.
@@ -257,16 +267,20 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
         VJ_TRY(col_norm.alloc(static_cast<size_t>(n)));
         VJ_TRY(r_k.alloc(static_cast<size_t>(m)));
         VJ_TRY(c_k.alloc(static_cast<size_t>(n)));
+        DeviceBuffer<int32_t> col_of;
+        VJ_TRY(col_of.alloc(static_cast<size_t>(nnz)));
+        k_expand_cols<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), col_of.get());
+        note_launch(1);
         VJ_CUDA(cudaMemsetAsync(sst, 0, sizeof(SetupState), st));
         for (int it = 0; it < o.ruiz_iterations; ++it) {
             k_col_inf<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), p.csc_val.get(), col_norm.get(), sst);
             k_row_inf<<<grid_for(m), kThreads, 0, st>>>(m, p.csr_ptr.get(), p.perm.get(), p.csc_val.get(),
                                                         row_norm.get(), sst);
-            k_ruiz_err<<<1, 1024, 0, st>>>(m, n, row_norm.get(), col_norm.get(), o.ruiz_tolerance, sst);
+            k_ruiz_err<<<1, 1, 0, st>>>(o.ruiz_tolerance, sst);
             k_scale_factors<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(), sst, 1);
             k_scale_factors<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(), sst, 1);
-            k_scale_matrix<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), lp.row_idx.get(), p.csc_val.get(),
-                                                             r_k.get(), c_k.get(), sst, 1);
+            k_scale_matrix<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, col_of.get(), lp.row_idx.get(),
+                                                                          p.csc_val.get(), r_k.get(), c_k.get(), sst, 1);
             VJ_LAUNCH_CHECK();
             note_launch(6);
         }
@@ -275,8 +289,8 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
             k_row_abs_sum<<<grid_for(m), kThreads, 0, st>>>(m, p.csr_ptr.get(), p.perm.get(), p.csc_val.get(), row_norm.get());
             k_scale_factors<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(), sst, 0);
             k_scale_factors<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(), sst, 0);
-            k_scale_matrix<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), lp.row_idx.get(), p.csc_val.get(),
-                                                             r_k.get(), c_k.get(), sst, 0);
+            k_scale_matrix<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, col_of.get(), lp.row_idx.get(),
+                                                                          p.csc_val.get(), r_k.get(), c_k.get(), sst, 0);
             VJ_LAUNCH_CHECK();
             note_launch(5);
         }
@@ -479,6 +493,21 @@ __global__ void k_rowblock_partition(int rows, const int64_t* __restrict__ ptr, 
     block_rows[b] = lo;
 }
 
+__global__ void k_tile_desc(int nb, const int64_t* __restrict__ ptr, const int32_t* __restrict__ block_rows,
+                            TileDesc* __restrict__ tiles) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const int r0 = block_rows[b], r1 = block_rows[b + 1];
+    int r_end = r1;
+    if (r1 > r0 && ptr[r1] - ptr[r1 - 1] > kTile) r_end = r1 - 1;
+    TileDesc d;
+    d.r0 = r0;
+    d.r_end = r_end > r0 ? r_end : r0;
+    d.e0 = r_end > r0 ? ptr[r0] : 0;
+    d.e1 = r_end > r0 ? ptr[r_end] : 0;
+    tiles[b] = d;
+}
+
 static vajra_status collect_long(const CsrView& v, int64_t long_len, DeviceBuffer<int32_t>& list, int* count,
                                  cudaStream_t st) {
     VJ_TRY(list.alloc(static_cast<size_t>(v.rows > 0 ? v.rows : 1)));
@@ -496,7 +525,7 @@ static vajra_status collect_long(const CsrView& v, int64_t long_len, DeviceBuffe
 }
 
 static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, DeviceBuffer<int32_t>& blocks,
-                             DeviceBuffer<int32_t>& rb_list, cudaStream_t st) {
+                             DeviceBuffer<TileDesc>& tiles, DeviceBuffer<int32_t>& rb_list, cudaStream_t st) {
     const double mean = v.rows > 0 ? static_cast<double>(v.nnz) / v.rows : 0.0;
     v.group = default_group(mean);
     int64_t long_len = static_cast<int64_t>(8.0 * mean);
@@ -515,6 +544,11 @@ static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, DeviceBuff
     VJ_LAUNCH_CHECK();
     note_launch(1);
     v.block_rows = blocks.get();
+    VJ_TRY(tiles.alloc(static_cast<size_t>(v.nb)));
+    k_tile_desc<<<grid_for(v.nb), kThreads, 0, st>>>(v.nb, v.ptr, v.block_rows, tiles.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
+    v.tiles = tiles.get();
     VJ_TRY(collect_long(v, kTile, rb_list, &v.rb_n_long, st));
     v.rb_long_rows = rb_list.get();
     return VAJRA_OK;
@@ -522,8 +556,8 @@ static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, DeviceBuff
 
 vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
     (void)lp;
-    VJ_TRY(plan_one(p.a, p.long_rows_a, p.rb_blocks_a, p.rb_long_a, st));
-    VJ_TRY(plan_one(p.at, p.long_rows_at, p.rb_blocks_at, p.rb_long_at, st));
+    VJ_TRY(plan_one(p.a, p.long_rows_a, p.rb_blocks_a, p.rb_tiles_a, p.rb_long_a, st));
+    VJ_TRY(plan_one(p.at, p.long_rows_at, p.rb_blocks_at, p.rb_tiles_at, p.rb_long_at, st));
     return VAJRA_OK;
 }
 

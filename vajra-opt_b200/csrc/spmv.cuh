@@ -67,6 +67,26 @@ __device__ __forceinline__ auto skip_rows_impl(const E& e, int r0, int r1, int) 
 template <class E>
 __device__ __forceinline__ bool skip_rows_impl(const E&, int, int, long) { return false; }
 
+// ----- optional two-phase epilogue ----------------------------------------------------
+// An epilogue may define `Pre pre(int row) const` -- every load it needs that does not
+// depend on the row sum -- and `void operator()(int row, Acc sum, const Pre&) const`.  The
+// fast kernels call pre() before the row's matrix loads, so the epilogue's vector loads are
+// in flight together with the SpMV's instead of after it (the epilogue's loads are otherwise
+// ordered behind its own stores).  Epilogues without pre() are called as epi(row, sum).
+struct NoPre {};
+template <class E>
+__device__ __forceinline__ auto epi_pre(const E& e, int row, int) -> decltype(e.pre(row)) { return e.pre(row); }
+template <class E>
+__device__ __forceinline__ NoPre epi_pre(const E&, int, long) { return NoPre{}; }
+template <class E, class Acc, class P>
+__device__ __forceinline__ auto epi_fin(const E& e, int row, Acc s, const P& p, int) -> decltype(e(row, s, p)) {
+    return e(row, s, p);
+}
+template <class E, class Acc, class P>
+__device__ __forceinline__ void epi_fin(const E& e, int row, Acc s, const P&, long) { e(row, s); }
+template <class E>
+using PreOf = decltype(epi_pre(*static_cast<const E*>(nullptr), 0, 0));
+
 // ----- epilogues usable by both families ---------------------------------------------
 template <typename T>
 struct EpiStore {
@@ -97,12 +117,43 @@ k_spmv_seq(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
 }
 
 // ----- fast family --------------------------------------------------------------------
+// The rows of lane-group block b: 256 / G consecutive rows, G lanes each.
+template <typename VV, typename VX, typename Acc, int G, class Epi>
+__device__ __forceinline__ void vec_block(int b, int rows, const int64_t* __restrict__ ptr,
+                                          const int32_t* __restrict__ idx, const VV* __restrict__ val,
+                                          const VX* __restrict__ x, int64_t long_len, const Epi& epi) {
+    const int lane = threadIdx.x & (G - 1);
+    const int row = (b * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x)) / G;
+    bool valid = row < rows;
+    int64_t s = 0, e = 0;
+    PreOf<Epi> pre{};
+    if (valid && lane == 0) pre = epi_pre(epi, row, 0);   // ahead of the row pointers
+    if (valid) {
+        s = ptr[row];
+        e = ptr[row + 1];
+        if (e - s > long_len || skip_rows_impl(epi, row, row + 1, 0)) valid = false;
+    }
+    Acc acc = Acc(0);
+    if (valid) {
+#pragma unroll 4
+        for (int64_t k = s + lane; k < e; k += G)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (valid && lane == 0) epi_fin(epi, row, acc, pre, 0);
+}
+
 // VV: stored value type, VX: dense-vector type, Acc: accumulation type.
+// CTAs [0, vec_blocks) take lane-group blocks: block blockIdx.x, or -- in list mode
+// (blk_list != null) -- blocks blk_list[t] for t = blockIdx.x, + vec_blocks, ... < *blk_count.
+// CTAs from vec_blocks on take one long row each.
 template <typename VV, typename VX, typename Acc, int G, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
            const VV* __restrict__ val, const VX* __restrict__ x, int64_t long_len,
-           const int32_t* __restrict__ long_rows, int vec_blocks, Epi epi) {
+           const int32_t* __restrict__ long_rows, int vec_blocks, const int32_t* __restrict__ blk_list,
+           const int* __restrict__ blk_count, Epi epi) {
     if (!epi.active()) return;
     if (static_cast<int>(blockIdx.x) >= vec_blocks) {
         // One CTA per long row.
@@ -118,40 +169,13 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
         if (threadIdx.x == 0) epi(row, v[0]);
         return;
     }
-    const int lane = threadIdx.x & (G - 1);
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-    bool valid = row < rows;
-    int64_t s = 0, e = 0;
-    if (valid) {
-        s = ptr[row];
-        e = ptr[row + 1];
-        if (e - s > long_len || skip_rows_impl(epi, row, row + 1, 0)) valid = false;
+    if (blk_list == nullptr) {
+        vec_block<VV, VX, Acc, G>(blockIdx.x, rows, ptr, idx, val, x, long_len, epi);
+        return;
     }
-    // Memory-level parallelism: each lane first issues a batch of kBatch index / value loads,
-    // then the kBatch independent gathers, then the FMAs (predicated at the row end), so a
-    // lane waits for two memory round trips per kBatch elements instead of two per element.
-    constexpr int kBatch = 4;
-    Acc acc = Acc(0);
-    if (valid) {
-        for (int64_t base = s + lane; base < e; base += static_cast<int64_t>(G) * kBatch) {
-            int ii[kBatch];
-            VV vv[kBatch];
-#pragma unroll
-            for (int t = 0; t < kBatch; ++t) {
-                const int64_t k = base + static_cast<int64_t>(t) * G;
-                ii[t] = k < e ? ld_stream(idx + k) : -1;
-                vv[t] = k < e ? ld_stream(val + k) : VV(0);
-            }
-            VX xx[kBatch];
-#pragma unroll
-            for (int t = 0; t < kBatch; ++t) xx[t] = ii[t] >= 0 ? ld_cached(x + ii[t]) : VX(0);
-#pragma unroll
-            for (int t = 0; t < kBatch; ++t) acc = fma(static_cast<Acc>(vv[t]), static_cast<Acc>(xx[t]), acc);
-        }
-    }
-#pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    if (valid && lane == 0) epi(row, acc);
+    const int cnt = *blk_count;
+    for (int t = blockIdx.x; t < cnt; t += vec_blocks)
+        vec_block<VV, VX, Acc, G>(blk_list[t], rows, ptr, idx, val, x, long_len, epi);
 }
 
 // ----- row-block family (shared-memory staging) ----------------------------------------
@@ -182,11 +206,91 @@ __device__ __forceinline__ void load4(const double* p, double (&v)[4]) {
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
+// A row block as the kernel reads it: rows [r0, r_end) and their entries [e0, e1) (the
+// block's last row is left out when it is longer than kTile).  Precomputed at set-up so a CTA
+// starts its stream loads after one dependent load instead of two.
+struct TileDesc {
+    long long e0, e1;
+    int r0, r_end;
+};
+
+// Resident CTAs per SM the row-block kernel is compiled for: with 4-byte values six (40
+// registers a thread) measured fastest; with 8-byte values four (64 registers; six spills).
+template <typename VV>
+constexpr int rowblock_min_blocks() { return sizeof(VV) == 4 ? 6 : 4; }
+
+// One row block (tile b).  Every exit before the first barrier is uniform over the CTA.
 template <typename VV, typename VX, typename Acc, class Epi>
-__global__ void __launch_bounds__(kThreads)
+__device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                              const VV* __restrict__ val, const VX* __restrict__ x,
+                                              const TileDesc* __restrict__ tiles, Acc* prod, int* med_rows,
+                                              int& n_med, const Epi& epi) {
+    const TileDesc td = tiles[b];
+    const int r0 = td.r0, r_end = td.r_end;
+    if (r0 >= r_end || skip_rows_impl(epi, r0, r_end, 0)) return;
+    const int64_t e0 = td.e0, e1 = td.e1;
+    // this thread's first row (the row it sums below): epilogue inputs and row bounds load
+    // now, alongside the block's stream
+    const int my_row = r0 + static_cast<int>(threadIdx.x);
+    PreOf<Epi> pre{};
+    int my_s = 0, my_e = 0;
+    if (my_row < r_end) {
+        pre = epi_pre(epi, my_row, 0);
+        my_s = static_cast<int>(ptr[my_row] - e0);
+        my_e = static_cast<int>(ptr[my_row + 1] - e0);
+    }
+    for (int64_t q = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x); q < e1; q += 4 * blockDim.x) {
+        int ii[4];
+        VV vv[4];
+        load4(idx + q, ii);
+        load4(val + q, vv);
+        Acc pr[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int64_t k = q + t;
+            pr[t] = (k >= e0 && k < e1) ? static_cast<Acc>(vv[t]) * static_cast<Acc>(ld_cached(x + ii[t])) : Acc(0);
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int64_t k = q + t;
+            if (k >= e0 && k < e1) prod[k - e0] = pr[t];
+        }
+    }
+    if (threadIdx.x == 0) n_med = 0;
+    __syncthreads();
+    for (int r = my_row; r < r_end; r += blockDim.x) {
+        const int s = r == my_row ? my_s : static_cast<int>(ptr[r] - e0);
+        const int e = r == my_row ? my_e : static_cast<int>(ptr[r + 1] - e0);
+        if (e - s > kMediumRow) {
+            med_rows[atomicAdd(&n_med, 1)] = r;
+            continue;
+        }
+        Acc acc = Acc(0);
+        for (int k = s; k < e; ++k) acc += prod[k];
+        if (r == my_row) epi_fin(epi, r, acc, pre, 0);
+        else epi(r, acc);
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int w = warp; w < n_med; w += blockDim.x >> 5) {
+        const int r = med_rows[w];
+        const int s = static_cast<int>(ptr[r] - e0), e = static_cast<int>(ptr[r + 1] - e0);
+        Acc acc = Acc(0);
+        for (int k = s + lane; k < e; k += 32) acc += prod[k];
+        acc = warp_reduce<OpSum>(acc);
+        if (lane == 0) epi(r, acc);
+    }
+}
+
+// CTAs [0, nb) take row blocks: block blockIdx.x, or -- in list mode (blk_list != null) --
+// blocks blk_list[t] for t = blockIdx.x, + nb, ... < *blk_count.  CTAs from nb on take one
+// row longer than kTile each.
+template <typename VV, typename VX, typename Acc, class Epi>
+__global__ void __launch_bounds__(kThreads, rowblock_min_blocks<VV>())
 k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const VV* __restrict__ val,
-                const VX* __restrict__ x, const int32_t* __restrict__ block_rows, int nb,
-                const int32_t* __restrict__ long_rows, Epi epi) {
+                const VX* __restrict__ x, const TileDesc* __restrict__ tiles, int nb,
+                const int32_t* __restrict__ long_rows, const int32_t* __restrict__ blk_list,
+                const int* __restrict__ blk_count, Epi epi) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Acc* prod = reinterpret_cast<Acc*>(smem_raw);
     __shared__ int med_rows[kMaxMediumRows];
@@ -205,65 +309,14 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
         if (threadIdx.x == 0) epi(row, v[0]);
         return;
     }
-    const int r0 = block_rows[blockIdx.x], r1 = block_rows[blockIdx.x + 1];
-    if (r0 >= r1) return;
-    int r_end = r1;
-    if (ptr[r1] - ptr[r1 - 1] > kTile) r_end = r1 - 1;
-    if (r0 >= r_end || skip_rows_impl(epi, r0, r_end, 0)) return;
-    const int64_t e0 = ptr[r0], e1 = ptr[r_end];
-    // A block stages fewer than 2 kTile entries, i.e. at most kQuads = 2 kTile / (4 kThreads)
-    // (+1 for alignment) aligned groups of four per thread.  All of a thread's index / value
-    // vector loads are issued first, then all its gathers, then the products are staged.
-    constexpr int kQuads = (2 * kTile) / (4 * kThreads) + 1;
-    const int64_t qbase = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x);
-    int ii[kQuads][4];
-    VV vv[kQuads][4];
-#pragma unroll
-    for (int u = 0; u < kQuads; ++u) {
-        const int64_t q = qbase + static_cast<int64_t>(u) * 4 * kThreads;
-        if (q < e1) {
-            load4(idx + q, ii[u]);
-            load4(val + q, vv[u]);
-        }
+    if (blk_list == nullptr) {
+        rowblock_tile<VV, VX, Acc>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        return;
     }
-    VX xx[kQuads][4];
-#pragma unroll
-    for (int u = 0; u < kQuads; ++u) {
-        const int64_t q = qbase + static_cast<int64_t>(u) * 4 * kThreads;
-#pragma unroll
-        for (int t = 0; t < 4; ++t)
-            xx[u][t] = (q < e1 && q + t >= e0 && q + t < e1) ? ld_cached(x + ii[u][t]) : VX(0);
-    }
-#pragma unroll
-    for (int u = 0; u < kQuads; ++u) {
-        const int64_t q = qbase + static_cast<int64_t>(u) * 4 * kThreads;
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int64_t k = q + t;
-            if (q < e1 && k >= e0 && k < e1) prod[k - e0] = static_cast<Acc>(vv[u][t]) * static_cast<Acc>(xx[u][t]);
-        }
-    }
-    if (threadIdx.x == 0) n_med = 0;
-    __syncthreads();
-    for (int r = r0 + threadIdx.x; r < r_end; r += blockDim.x) {
-        const int s = static_cast<int>(ptr[r] - e0), e = static_cast<int>(ptr[r + 1] - e0);
-        if (e - s > kMediumRow) {
-            med_rows[atomicAdd(&n_med, 1)] = r;
-            continue;
-        }
-        Acc acc = Acc(0);
-        for (int k = s; k < e; ++k) acc += prod[k];
-        epi(r, acc);
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int w = warp; w < n_med; w += blockDim.x >> 5) {
-        const int r = med_rows[w];
-        const int s = static_cast<int>(ptr[r] - e0), e = static_cast<int>(ptr[r + 1] - e0);
-        Acc acc = Acc(0);
-        for (int k = s + lane; k < e; k += 32) acc += prod[k];
-        acc = warp_reduce<OpSum>(acc);
-        if (lane == 0) epi(r, acc);
+    const int cnt = *blk_count;
+    for (int t = blockIdx.x; t < cnt; t += nb) {
+        rowblock_tile<VV, VX, Acc>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        __syncthreads();   // the tile's shared state is reused by the next one
     }
 }
 
@@ -280,24 +333,34 @@ struct CsrView {
     const int32_t* long_rows = nullptr; // device list of those rows
     int n_long = 0;
     const int32_t* block_rows = nullptr;  // row-block kernel: nb + 1 block boundaries
+    const TileDesc* tiles = nullptr;      // and the nb blocks as the kernel reads them
     int nb = 0;
     const int32_t* rb_long_rows = nullptr;  // rows longer than kTile
     int rb_n_long = 0;
+    // List mode (the batched solver): only the blocks blk_list[0, *blk_count) -- lane-group
+    // blocks of `group`, or row blocks for group 0 -- are computed, by blk_grid persistent CTAs.
+    const int32_t* blk_list = nullptr;
+    const int* blk_count = nullptr;
+    int blk_grid = 0;
 };
 
 template <typename VV, typename VX, typename Acc, class Epi>
 inline void launch_rowblock(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     const size_t smem = sizeof(Acc) * 2 * kTile;
-    k_spmv_rowblock<VV, VX, Acc, Epi><<<a.nb + a.rb_n_long, kThreads, smem, st>>>(
-        a.ptr, a.idx, val, x, a.block_rows, a.nb, a.rb_long_rows, epi);
+    const int nb = a.blk_list ? a.blk_grid : a.nb;
+    k_spmv_rowblock<VV, VX, Acc, Epi><<<nb + a.rb_n_long, kThreads, smem, st>>>(
+        a.ptr, a.idx, val, x, a.tiles, nb, a.rb_long_rows, a.blk_list, a.blk_count, epi);
     note_launch();
 }
 
+// Lane-group blocks of the grouped-lane kernel at G lanes per row.
+inline int vec_block_count(int rows, int G) { return static_cast<int>(grid_for(static_cast<int64_t>(rows) * G)); }
+
 template <typename VV, typename VX, typename Acc, int G, class Epi>
 inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
-    const int vec_blocks = static_cast<int>(grid_for(static_cast<int64_t>(a.rows) * G));
+    const int vec_blocks = a.blk_list ? a.blk_grid : vec_block_count(a.rows, G);
     k_spmv_vec<VV, VX, Acc, G, Epi><<<vec_blocks + a.n_long, kThreads, 0, st>>>(
-        a.rows, a.ptr, a.idx, val, x, a.long_len, a.long_rows, vec_blocks, epi);
+        a.rows, a.ptr, a.idx, val, x, a.long_len, a.long_rows, vec_blocks, a.blk_list, a.blk_count, epi);
     note_launch();
 }
 
@@ -307,7 +370,7 @@ inline void launch_spmv_t(const CsrView& a, const VV* val, const VX* x, Epi epi,
     if (a.rows <= 0) return;
     switch (a.group) {
         case 0:
-            if (a.block_rows) { launch_rowblock<VV, VX, Acc>(a, val, x, epi, st); break; }
+            if (a.tiles) { launch_rowblock<VV, VX, Acc>(a, val, x, epi, st); break; }
             launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st);
             break;
         case 1: launch_vec_g<VV, VX, Acc, 1>(a, val, x, epi, st); break;
