@@ -55,9 +55,15 @@ def parse():
     ap.add_argument("--profile-iters", type=int, default=0,
                     help="profiling aid: one solve capped at this many iterations, then exit (for ncu)")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--shapes", default=None,
+                    help="profiling: fixed SpMV launch shapes 'A,AT' (-1 row block, 1..32 lanes per row) "
+                         "instead of autotuning, whose timings a profiler would distort")
     ap.add_argument("--batch", type=int, default=0,
                     help="batched workload instead: this many config-0-style LPs (m log-uniform on "
                          "[100, 20000]), one batched solve vs the same LPs solved one after another")
+    ap.add_argument("--study", choices=["small", "flow", "adjoint"], default=None,
+                    help="one JSON line for another workload: small = 2000x5000 planted LP, flow = min-cost "
+                         "flow 200k nodes x 1.5M arcs, adjoint = 256 x (1000x3000) unrolled-PDHG gradients vs FD")
     ap.add_argument("--batch-sequential", type=int, default=-1,
                     help="how many of the LPs to time sequentially (default all; the rate is per solve)")
     return ap.parse_args()
@@ -120,6 +126,132 @@ def run_batch_bench(args, world=1, rank=0, dist=None):
                               "optimal": seq_ok}
         line["speedup"] = seq_total / batch_wall
     print(json.dumps(line))
+    return 0
+
+
+def run_study(args, local=0):
+    """Solve-time / SpMV-bandwidth / adjoint-accuracy line for the other configurations."""
+    import numpy as np
+    import vajra_pdhg as V
+    from vajra_pdhg import workloads as W
+    from vajra_pdhg.kkt import relative_kkt
+    if args.study == "adjoint":
+        return run_adjoint_study(args)
+    lp = W.random_planted(2000, 5000, 8, seed=0) if args.study == "small" else W.min_cost_flow()
+    planted = getattr(lp, "planted_objective", None)
+    out = {"study": args.study, "workload": lp.name, "m": lp.num_rows, "n": lp.num_cols, "nnz": int(lp.nnz),
+           "data": "synthetic", "tolerance": "FP64 relative KKT <= 1e-6 on the original LP"}
+    for name, prec in (("mixed", V.PREC_MIXED), ("fp64", V.PREC_FP64)):
+        s = V.Solver(lp, precision=prec, device=local)
+        s.run()                                  # warm (autotuning, graph capture)
+        runs = [s.run() for _ in range(max(1, args.steps))]
+        s.close()
+        r = runs[-1]
+        k = relative_kkt(lp, r["x"], r["y"])
+        out[name] = {"time_s": statistics.mean(x["device_time_sec"] for x in runs), "status": r["status_name"],
+                     "iterations": r["iterations"], "fp32_iterations": r["fp32_iterations"],
+                     "fp64_iterations": r["fp64_iterations"],
+                     "device_rel_kkt": r["rel_kkt"], "host_rel_kkt": k["rel_kkt"],
+                     "objective": r["objective_value"],
+                     "primal_kernel": {"us": r["primal_kernel_us"], "gbs": r["primal_kernel_bytes"] / max(1e-9, r["primal_kernel_us"]) / 1e3},
+                     "dual_kernel": {"us": r["dual_kernel_us"], "gbs": r["dual_kernel_bytes"] / max(1e-9, r["dual_kernel_us"]) / 1e3},
+                     "spmv_groups": [r["spmv_group_a"], r["spmv_group_at"]]}
+        if planted is not None:
+            out[name]["objective_rel_err_vs_planted"] = abs(r["objective_value"] - planted) / (1 + abs(planted))
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["time_s"] / out["mixed"]["time_s"]
+    peak, kind = load_peaks()
+    out["hbm_peak_gbs"] = {"value": peak, "kind": kind}
+    if not args.no_cpu_baseline:
+        from oracle import bindings as B
+        if B.ref_available():
+            if args.study == "small":      # the reference CPU PDHG run to its own termination
+                t0 = time.perf_counter()
+                r = B.ref_solve(lp, iteration_limit=1_000_000, tolerance=1e-6, gap_tolerance=1e-6)
+                out["cpu_reference"] = {"wall_s": time.perf_counter() - t0, "status": r["status_name"],
+                                        "iterations": r["iterations"], "primal_residual": r["primal_residual"],
+                                        "dual_residual": r["dual_residual"], "objective": r["objective_value"],
+                                        "cores": 1}
+                if planted is not None:
+                    out["cpu_reference"]["objective_rel_err_vs_planted"] = \
+                        abs(r["objective_value"] - planted) / (1 + abs(planted))
+            else:                          # a fixed 1000 iterations
+                rc = reference_cpu(lp, 1000)
+                out["cpu_reference"] = {"per_iteration_us": rc["per_iter_s"] * 1e6, "setup_s": rc["setup_s"],
+                                        "cores": 1, "sample": "1000 iterations"}
+    print(json.dumps(out))
+    return 0
+
+
+def run_adjoint_study(args):
+    """Config 4: 256 LPs of 1000 x 3000; gradients of L_i = (w + c).x_i(K) over K = 2000
+    unrolled iterations (checkpoint every 100), FP32 and FP64 forms, against FP64 central
+    differences along random directions, instance by instance.
+
+    The unrolled map is piecewise affine in (c, b): a pair (instance, direction) whose forward
+    and backward differences disagree beyond rounding has an active-set change within +-h and
+    no derivative to compare; such pairs are counted, not compared.  With 2000 iterations of
+    4000 projections each, almost every pair crosses one at h = 1e-6, so smaller steps are
+    reported as well (rounding of the FP64 losses bounds how small h can go)."""
+    import numpy as np
+    from vajra_pdhg import workloads as W
+    from vajra_pdhg.autograd import PREC_FP64, PREC_MIXED, unrolled
+    lps = [W.random_planted(1000, 3000, 8, seed=1000 + i) for i in range(256)]
+    rng = np.random.default_rng(4)
+    N = sum(lp.num_cols for lp in lps)
+    M = sum(lp.num_rows for lp in lps)
+    w = rng.standard_normal(N)
+    opts = dict(iterations=2000, checkpoint_every=100)
+    timing, grads = {}, {}
+    for name, prec in (("fp32", PREC_MIXED), ("fp64", PREC_FP64)):
+        unrolled(lps[:4], w[: sum(lp.num_cols for lp in lps[:4])], precision=prec, **opts)   # warm
+        t0 = time.perf_counter()
+        grads[name] = unrolled(lps, w, precision=prec, **opts)
+        timing[name] = time.perf_counter() - t0
+    coff = np.cumsum([0] + [lp.num_cols for lp in lps])
+    roff = np.cumsum([0] + [lp.num_rows for lp in lps])
+    c0 = np.concatenate([lp.c for lp in lps])
+    b0 = np.concatenate([lp.row_lower for lp in lps])
+
+    def losses(h, dc, db):
+        pert = []
+        for i, lp in enumerate(lps):
+            q = W.LP(**{**lp.__dict__})
+            q.c = c0[coff[i]:coff[i + 1]] + h * dc[coff[i]:coff[i + 1]]
+            b = b0[roff[i]:roff[i + 1]] + h * db[roff[i]:roff[i + 1]]
+            q.row_lower = b.copy()
+            q.row_upper = b.copy()
+            pert.append(q)
+        return unrolled(pert, w, gradients=False, precision=PREC_FP64, **opts)["loss"]
+
+    f0 = losses(0.0, np.zeros(N), np.zeros(M))
+    eps = np.finfo(np.float64).eps
+    per_h = {}
+    for h, ndir in ((1e-6, 32), (1e-8, 32), (1e-9, 64)):
+        errs = {"fp32": [], "fp64": []}
+        kinks = 0
+        for _ in range(ndir):
+            dc = rng.standard_normal(N)
+            db = rng.standard_normal(M)
+            fp, fm = losses(h, dc, db), losses(-h, dc, db)
+            fwd, bwd, central = (fp - f0) / h, (f0 - fm) / h, (fp - fm) / (2 * h)
+            for i in range(len(lps)):
+                noise = 16 * eps * (abs(f0[i]) + abs(fp[i]) + abs(fm[i])) / h
+                if abs(fwd[i] - bwd[i]) > 1e-4 * max(abs(fwd[i]), abs(bwd[i])) + noise:
+                    kinks += 1
+                    continue
+                for name, g in grads.items():
+                    gb = g["grad_row_lower"][roff[i]:roff[i + 1]] + g["grad_row_upper"][roff[i]:roff[i + 1]]
+                    adj = g["grad_c"][coff[i]:coff[i + 1]] @ dc[coff[i]:coff[i + 1]] + gb @ db[roff[i]:roff[i + 1]]
+                    errs[name].append(abs(adj - central[i]) / max(1e-12, abs(central[i])))
+        per_h[f"{h:g}"] = {"directions": ndir, "pairs": ndir * len(lps), "kink_pairs": kinks,
+                           "compared_pairs": ndir * len(lps) - kinks,
+                           "max_rel_err": {k: (max(v) if v else None) for k, v in errs.items()},
+                           "p99_rel_err": {k: (float(np.percentile(v, 99)) if v else None) for k, v in errs.items()},
+                           "median_rel_err": {k: (float(np.median(v)) if v else None) for k, v in errs.items()}}
+    out = {"study": "adjoint", "workload": "256 x random_planted(1000, 3000, 8 nnz/col), seeds 1000..1255",
+           "unrolled_iterations": 2000, "checkpoint_every": 100, "fd": "FP64 central differences per instance",
+           "adjoint_time_s": timing, "by_step": per_h, "target": "<= 1e-4 relative"}
+    print(json.dumps(out))
     return 0
 
 
@@ -291,12 +423,18 @@ def main():
 
     if args.batch > 0:
         return run_batch_bench(args, world, rank, dist)
+    if args.study:
+        return run_study(args, local) if rank == 0 else 0
     torch.cuda.set_device(local)
     lp = W.random_large(args.rows, args.cols, seed=args.seed + rank)
     if args.profile_iters > 0:
         prec = V.PREC_MIXED if args.profile_precision == "mixed" else V.PREC_FP64
+        shapes = {}
+        if args.shapes:
+            sa, sat = (int(v) for v in args.shapes.split(","))
+            shapes = dict(spmv_shape_a=sa, spmv_shape_at=sat, autotune=0)
         r = V.solve(lp, precision=prec, iteration_limit=args.profile_iters, device=local,
-                    mixed_switch_tolerance=0.0, mixed_stall_checks=0)
+                    mixed_switch_tolerance=0.0, mixed_stall_checks=0, **shapes)
         print(json.dumps({"profile_iters": r["iterations"], "status": r["status_name"], "rel_kkt": r["rel_kkt"],
                           "groups": [r["spmv_group_a"], r["spmv_group_at"]],
                           "primal_us": r["primal_kernel_us"], "dual_us": r["dual_kernel_us"],

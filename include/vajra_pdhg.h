@@ -29,7 +29,7 @@ extern "C" {
 
 /* Layout version of the structs below.  A caller compiled against one version must not call
  * a library of another: compare with vajra_abi_version() before the first call. */
-#define VAJRA_ABI_VERSION 3
+#define VAJRA_ABI_VERSION 4
 
 typedef int32_t vajra_status;
 enum {
@@ -123,7 +123,11 @@ typedef struct vajra_opts {
     double step_safety;         /* eta = step_safety / ||A||_2 (0.99)                    */
     int32_t restart_metric;     /* 0: primal-weighted KKT of T(z); 1: fixed-point residual
                                    sqrt(omega ||x+ - x||^2 + ||y+ - y||^2 / omega)          */
-    int32_t reserved[5];
+    int32_t spmv_shape_a;       /* HALPERN launch shape of the A x SpMV: 0 autotune (>= 2^20
+                                   entries) or the set-up heuristic, -1 row-block kernel,
+                                   1..32 lanes per row (1, 2, 4, 8, 16, 32)                */
+    int32_t spmv_shape_at;      /* the same for the A^T y SpMV                           */
+    int32_t reserved[3];
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and

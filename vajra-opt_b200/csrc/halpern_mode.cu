@@ -539,7 +539,10 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     const double gamma = o.reflection;
     CsrView a64 = p.a, at64 = p.at;
     CsrView a32 = p.a, at32 = p.at;
-    if (o.autotune && (!(h->tuned & 2) || (mixed && !(h->tuned & 1)))) {
+    // Below ~1M entries a solve is launch-bound and the timing runs would cost more than any
+    // shape saves: the set-up heuristic (lanes per row from the mean row length) stays.
+    constexpr int64_t kAutotuneMinNnz = int64_t(1) << 20;
+    if (o.autotune && nnz >= kAutotuneMinNnz && (!(h->tuned & 2) || (mixed && !(h->tuned & 1)))) {
         HState tune = init;
         if (mixed && !(h->tuned & 1)) {
             tune.phase = 0;
@@ -560,12 +563,20 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             h->tuned |= 2;
         }
     }
-    if (o.autotune) {
+    if (h->tuned & 1) {
         a32.group = h->tuned_a32;
         at32.group = h->tuned_at32;
+    }
+    if (h->tuned & 2) {
         a64.group = h->tuned_a64;
         at64.group = h->tuned_at64;
     }
+    auto forced = [](int32_t shape, CsrView& v32, CsrView& v64) {   // caller-fixed shapes
+        if (shape == -1 || shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16 || shape == 32)
+            v32.group = v64.group = shape == -1 ? 0 : shape;
+    };
+    forced(o.spmv_shape_a, a32, a64);
+    forced(o.spmv_shape_at, at32, at64);
     const CsrView& a_it = mixed ? a32 : a64;     // shapes reported for the dominant phase
     const CsrView& at_it = mixed ? at32 : at64;
 
