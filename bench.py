@@ -498,7 +498,9 @@ def main():
         d2h = 8 * (2 * lp.num_cols + 2 * lp.num_rows)
         e2e = {"value": max_over_ranks(statistics.mean(e2e_times)), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "status": r["status_name"], "rel_kkt": r["rel_kkt"]}
+               "status": r["status_name"], "rel_kkt": r["rel_kkt"],
+               "last_call_breakdown_s": {k: r[k] for k in ("upload_time_sec", "setup_time_sec", "iteration_time_sec",
+                                                           "download_time_sec", "total_time_sec", "device_time_sec")}}
 
     # ---- roofline of the dominant iteration kernel ----------------------------------
     peak, peak_kind = load_peaks()

@@ -29,7 +29,7 @@ extern "C" {
 
 /* Layout version of the structs below.  A caller compiled against one version must not call
  * a library of another: compare with vajra_abi_version() before the first call. */
-#define VAJRA_ABI_VERSION 4
+#define VAJRA_ABI_VERSION 5
 
 typedef int32_t vajra_status;
 enum {
@@ -110,11 +110,12 @@ typedef struct vajra_opts {
     int32_t ruiz_iterations;    /* 10 (tol::kMaxRuizIterations)                          */
     double reflection;          /* HALPERN: reflection coefficient of the Halpern step   */
     double mixed_switch_tolerance; /* MIXED: FP32 phase hands over to FP64 below this
-                                      relative KKT (or when FP32 stalls)                 */
+                                      relative KKT (2e-6), or when FP32 stalls            */
     int32_t device;             /* CUDA device ordinal                                   */
     int32_t autotune;           /* 1 = time SpMV variants at set-up and keep the fastest */
     int32_t verbose;            /* 1 = one line per check on stderr                      */
-    int32_t mixed_stall_checks; /* MIXED: hand over when 10 checks gained < 5 % (0 = never) */
+    int32_t mixed_stall_checks; /* MIXED: hand over when the relative KKT gained < 2 % over
+                                   this many checks (20; 0 = never; at most 31)          */
     /* HALPERN restart and step parameters */
     double restart_sufficient;  /* restart when weighted KKT <= this x its restart value (0.2) */
     double restart_necessary;   /* ... or <= this x and rising (0.8)                     */
@@ -127,7 +128,11 @@ typedef struct vajra_opts {
                                    entries) or the set-up heuristic, -1 row-block kernel,
                                    1..32 lanes per row (1, 2, 4, 8, 16, 32)                */
     int32_t spmv_shape_at;      /* the same for the A^T y SpMV                           */
-    int32_t reserved[3];
+    double mixed_reflection;    /* MIXED: reflection coefficient of the FP32 phase (0.8); the
+                                   FP64 phase uses `reflection`.  Below 1 the reflected step is
+                                   averaged, which keeps FP32 rounding noise from building up
+                                   within a restart epoch                                 */
+    int32_t reserved[2];
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and

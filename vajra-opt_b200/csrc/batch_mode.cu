@@ -32,6 +32,9 @@ struct BatchArrays {      // device struct of arrays, B entries each
     double* kkt_start; double* kkt_prev;
     double* rel_p; double* rel_d; double* rel_gap; double* rel_kkt; double* pobj; double* dobj;
     double* bnorm; double* cnorm; double* offset_min; double* lambda;
+    double* inv_sigma;    // 1 / sigma
+    double* hw;           // Halpern weights of the current chunk, 2 hw_len per instance:
+    int hw_len;           // hw[i 2 hw_len + 2 kk] = (k+1)/(k+2), [.. + 1] = 1/(k+2), k = k_base + kk
     long long* k_base; long long* total;
     int* done; int* status; int* restart_count; int* restart_flag;
 };
@@ -40,6 +43,16 @@ struct BatchCounters {
     int active;
     int pad;
 };
+
+__device__ __forceinline__ void instance_weights(const BatchArrays& S, int i) {
+    const long long kb = S.k_base[i];
+    double* w = S.hw + static_cast<size_t>(i) * 2 * S.hw_len;
+    for (int kk = 0; kk < S.hw_len; ++kk) {
+        const double k = static_cast<double>(kb + kk);
+        w[2 * kk] = (k + 1.0) / (k + 2.0);
+        w[2 * kk + 1] = 1.0 / (k + 2.0);
+    }
+}
 
 __device__ __forceinline__ bool any_active(const int* done, const int* inst, int r0, int r1) {
     const int a = inst[r0], b = inst[r1 - 1];
@@ -56,14 +69,16 @@ struct EpiBPrimal {
     double gamma;
     int kk, write_cand;
     // two-phase (spmv.cuh): the instance lookups and vector loads go out before the SpMV's
-    struct Pre { double k, tau, xo, c, cl, cu, x0; int done; };
+    struct Pre { double w1, w0, tau, xo, c, cl, cu, x0; int done; };
     __device__ bool active() const { return true; }
     __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, col_inst, r0, r1); }
     __device__ Pre pre(int j) const {
         const int i = __ldg(col_inst + j);
         Pre p;
         p.done = S.done[i];
-        p.k = static_cast<double>(S.k_base[i] + kk);
+        const double* w = S.hw + static_cast<size_t>(i) * 2 * S.hw_len + 2 * kk;
+        p.w1 = w[0];
+        p.w0 = w[1];
         p.tau = S.tau[i];
         p.xo = x[j];
         p.c = __ldg(c + j);
@@ -74,11 +89,10 @@ struct EpiBPrimal {
     }
     __device__ void operator()(int j, double v, const Pre& p) const {
         if (p.done) return;
-        const double w1 = (p.k + 1.0) / (p.k + 2.0), w0 = 1.0 / (p.k + 2.0);
         double xp = p.xo - p.tau * (p.c + v);
         xp = xp < p.cl ? p.cl : (xp > p.cu ? p.cu : xp);
         xb[j] = xp + xp - p.xo;
-        x[j] = w1 * ((1.0 + gamma) * xp - gamma * p.xo) + w0 * p.x0;
+        x[j] = p.w1 * ((1.0 + gamma) * xp - gamma * p.xo) + p.w0 * p.x0;
         if (write_cand) xc[j] = xp;
     }
     __device__ void operator()(int j, double v) const { (*this)(j, v, pre(j)); }
@@ -91,15 +105,18 @@ struct EpiBDual {
     BatchArrays S;
     double gamma;
     int kk, write_cand;
-    struct Pre { double k, sigma, yo, rl, ru, y0; int done; };
+    struct Pre { double w1, w0, sigma, inv_sigma, yo, rl, ru, y0; int done; };
     __device__ bool active() const { return true; }
     __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, row_inst, r0, r1); }
     __device__ Pre pre(int r) const {
         const int i = __ldg(row_inst + r);
         Pre p;
         p.done = S.done[i];
-        p.k = static_cast<double>(S.k_base[i] + kk);
+        const double* w = S.hw + static_cast<size_t>(i) * 2 * S.hw_len + 2 * kk;
+        p.w1 = w[0];
+        p.w0 = w[1];
         p.sigma = S.sigma[i];
+        p.inv_sigma = S.inv_sigma[i];
         p.yo = y[r];
         p.rl = __ldg(rl + r);
         p.ru = __ldg(ru + r);
@@ -108,13 +125,12 @@ struct EpiBDual {
     }
     __device__ void operator()(int r, double w, const Pre& p) const {
         if (p.done) return;
-        const double w1 = (p.k + 1.0) / (p.k + 2.0), w0 = 1.0 / (p.k + 2.0);
         const double sg = p.sigma;
         const double yh = p.yo + sg * w;
-        double q = yh / sg;
+        double q = yh * p.inv_sigma;
         q = q < p.rl ? p.rl : (q > p.ru ? p.ru : q);
         const double yp = yh - sg * q;
-        y[r] = w1 * ((1.0 + gamma) * yp - gamma * p.yo) + w0 * p.y0;
+        y[r] = p.w1 * ((1.0 + gamma) * yp - gamma * p.yo) + p.w0 * p.y0;
         if (write_cand) yc[r] = yp;
     }
     __device__ void operator()(int r, double w) const { (*this)(r, w, pre(r)); }
@@ -292,6 +308,7 @@ __global__ void k_bcontrol(const double* __restrict__ part, BControl cp, BatchAr
             S.omega[i] = exp(th * log(dy / dx) + (1.0 - th) * log(omega));
             S.tau[i] = S.eta[i] / S.omega[i];
             S.sigma[i] = S.eta[i] * S.omega[i];
+            S.inv_sigma[i] = 1.0 / S.sigma[i];
         }
         S.k_base[i] = 0;
         S.kkt_start[i] = wk;
@@ -301,6 +318,7 @@ __global__ void k_bcontrol(const double* __restrict__ part, BControl cp, BatchAr
     } else {
         S.k_base[i] = k_in;
     }
+    instance_weights(S, i);
 }
 
 __global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restrict__ done, BatchCounters* out) {
@@ -350,11 +368,13 @@ k_binit(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, cons
     const double omega = (bs > 1e-10 && csn > 1e-10) ? csn / bs : 1.0;
     S.bnorm[inst] = bn; S.cnorm[inst] = cn;
     S.eta[inst] = eta; S.omega[inst] = omega; S.tau[inst] = eta / omega; S.sigma[inst] = eta * omega;
+    S.inv_sigma[inst] = 1.0 / (eta * omega);
     S.kkt_start[inst] = -1.0; S.kkt_prev[inst] = -1.0;
     S.offset_min[inst] = sense[inst] ? -offsets[inst] : offsets[inst];
     S.k_base[inst] = 0; S.total[inst] = 0;
     S.done[inst] = 0; S.status[inst] = 0; S.restart_count[inst] = 0; S.restart_flag[inst] = 0;
     S.rel_kkt[inst] = 1e30;
+    instance_weights(S, inst);
 }
 
 __global__ void k_binit_iterates(int m, int n, const double* __restrict__ cl, const double* __restrict__ cu,
@@ -528,13 +548,19 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     DeviceBuffer<double> dd;
     DeviceBuffer<long long> dl;
     DeviceBuffer<int> di;
-    VJ_TRY(dd.alloc(16 * static_cast<size_t>(count)));
+    VJ_TRY(dd.alloc(17 * static_cast<size_t>(count)));
+    const int K = o.check_frequency > 0 ? o.check_frequency : 64;
+    DeviceBuffer<double> d_hw;
+    VJ_TRY(d_hw.alloc(2 * static_cast<size_t>(K) * count));
     VJ_TRY(dl.alloc(2 * static_cast<size_t>(count)));
     VJ_TRY(di.alloc(4 * static_cast<size_t>(count)));
     BatchArrays S;
     double** fields[] = {&S.omega, &S.eta, &S.tau, &S.sigma, &S.kkt_start, &S.kkt_prev, &S.rel_p, &S.rel_d,
-                         &S.rel_gap, &S.rel_kkt, &S.pobj, &S.dobj, &S.bnorm, &S.cnorm, &S.offset_min, &S.lambda};
-    for (int q = 0; q < 16; ++q) *fields[q] = dd.get() + static_cast<size_t>(q) * count;
+                         &S.rel_gap, &S.rel_kkt, &S.pobj, &S.dobj, &S.bnorm, &S.cnorm, &S.offset_min, &S.lambda,
+                         &S.inv_sigma};
+    for (int q = 0; q < 17; ++q) *fields[q] = dd.get() + static_cast<size_t>(q) * count;
+    S.hw = d_hw.get();
+    S.hw_len = K;
     S.k_base = dl.get(); S.total = dl.get() + count;
     S.done = di.get(); S.status = di.get() + count; S.restart_count = di.get() + 2 * count;
     S.restart_flag = di.get() + 3 * count;
@@ -635,7 +661,6 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     bc.pw_smoothing = o.primal_weight_smoothing;
     bc.count = count;
     const double gamma = o.reflection;
-    const int K = o.check_frequency > 0 ? o.check_frequency : 64;
     int64_t graph_kernels = 0;
 
     auto enqueue_chunk = [&](int len) {

@@ -181,11 +181,12 @@ void vajra_default_opts(vajra_opts* o) {
     o->pock_chambolle = 1;
     o->ruiz_iterations = 10;
     o->reflection = 1.0;
-    o->mixed_switch_tolerance = 1e-5;
+    o->mixed_switch_tolerance = 2e-6;
+    o->mixed_reflection = 0.8;
     o->device = 0;
     o->autotune = 1;
     o->verbose = 0;
-    o->mixed_stall_checks = 10;
+    o->mixed_stall_checks = 20;
     o->restart_sufficient = 0.2;
     o->restart_necessary = 0.8;
     o->restart_artificial = 0.36;

@@ -180,7 +180,7 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
         bool stalled = false;
         if (w > 0 && hn >= w) {
             const double old = st->hist[(hn - w) % kHist];
-            stalled = rel > 0.95 * old;
+            stalled = rel > 0.98 * old;
         }
         st->hist[hn % kHist] = rel;
         st->hist_n = hn + 1;
@@ -206,6 +206,7 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
             st->omega = exp(th * log(dy / dx) + (1.0 - th) * log(omega));
             st->tau = st->eta / st->omega;
             st->sigma = st->eta * st->omega;
+            st->inv_sigma = 1.0 / st->sigma;
         }
         st->k_base = 0;
         st->kkt_start = wk;
@@ -220,7 +221,8 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
 template <typename T>
 __global__ void k_halpern_restart(int m, int n, const T* __restrict__ xc, const T* __restrict__ yc, T* __restrict__ x,
                                   T* __restrict__ x0, T* __restrict__ y, T* __restrict__ y0, double* __restrict__ x_last,
-                                  double* __restrict__ y_last, const HState* st) {
+                                  double* __restrict__ y_last, const HState* st, int len, double* __restrict__ hw) {
+    if (blockIdx.x == 0) halpern_weights(st, len, hw, threadIdx.x, blockDim.x);   // for the next chunk
     if (!st->restart_flag) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { const T v = xc[i]; x[i] = v; x0[i] = v; x_last[i] = static_cast<double>(v); }
@@ -349,21 +351,23 @@ struct Phase {
 
 // `timed`: bracket the two kernels with event-record nodes (captured into the chunk graph).
 template <typename T>
-void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, double gamma, int kk,
+void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, const double* hw, double gamma, int kk,
                        int write_cand, bool timed, cudaStream_t st) {
     if (timed) cudaEventRecordWithFlags(ph.ev[0], st, cudaEventRecordExternal);
     launch_spmv_t<T, T, T>(at, ph.csc_val, ph.y.get(),
                            EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                         ph.xc.get(), ph.xprev.get(), S, gamma, kk, ph.phase, write_cand}, st);
+                                         ph.xc.get(), ph.xprev.get(), S, hw, gamma, kk, ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[1], st, cudaEventRecordExternal);
     launch_spmv_t<T, T, T>(a, ph.csr_val, ph.xb.get(),
-                           EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, gamma, kk,
+                           EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, gamma, kk,
                                        ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[2], st, cudaEventRecordExternal);
 }
 
 struct CheckBuffers {
     DeviceBuffer<double> ax, aty, part_r, part_c, x_last, y_last;
+    DeviceBuffer<double> hw;   // Halpern weights of the current chunk (2 per iteration)
+    int hw_len = 0;            // iterations a chunk can hold
 };
 
 template <typename T>
@@ -381,7 +385,7 @@ void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const 
     const int mx = ph.m > ph.n ? ph.m : ph.n;
     k_halpern_restart<T><<<grid_for(mx), kThreads, 0, st>>>(ph.m, ph.n, ph.xc.get(), ph.yc.get(), ph.x.get(),
                                                             ph.x0.get(), ph.y.get(), ph.y0.get(), cb.x_last.get(),
-                                                            cb.y_last.get(), S);
+                                                            cb.y_last.get(), S, cb.hw_len, cb.hw.get());
     note_launch(4);
 }
 
@@ -391,7 +395,7 @@ void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrV
                    ControlParams cp, bool capturing, cudaStream_t st) {
     // Event-record nodes (cudaEventRecordExternal) exist only inside a stream capture.
     for (int kk = 0; kk < len; ++kk)
-        enqueue_iteration(ph, a, at, S, gamma, kk, kk == len - 1 ? 1 : 0, kk == 0 && capturing, st);
+        enqueue_iteration(ph, a, at, S, cb.hw.get(), gamma, kk, kk == len - 1 ? 1 : 0, kk == 0 && capturing, st);
     cp.len = len;
     cp.phase = ph.phase;
     enqueue_check(ph, a64, at64, p, lp, cb, S, cp, st);
@@ -401,8 +405,11 @@ void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrV
 // with their real epilogues and keeps the fastest per matrix.  `tune_state` is a scratch
 // state whose phase is the tuned one; the iterates it scribbles on are re-initialised after.
 template <typename T>
-vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* tune_state, double gamma,
-                                cudaStream_t st) {
+vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* tune_state, const CheckBuffers& cb,
+                                double gamma, cudaStream_t st) {
+    const double* hw = cb.hw.get();
+    k_halpern_weights<<<1, kThreads, 0, st>>>(tune_state, cb.hw_len, cb.hw.get());
+    note_launch(1);
     cudaEvent_t e0, e1;
     VJ_CUDA(cudaEventCreate(&e0));
     VJ_CUDA(cudaEventCreate(&e1));
@@ -429,12 +436,12 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
     VJ_TRY(time_shapes(at, [&](const CsrView& t) {
         launch_spmv_t<T, T, T>(t, ph.csc_val, ph.y.get(),
                                EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                             ph.xc.get(), ph.xprev.get(), tune_state, gamma, 0, ph.phase, 0}, st);
+                                             ph.xc.get(), ph.xprev.get(), tune_state, hw, gamma, 0, ph.phase, 0}, st);
     }));
     VJ_TRY(time_shapes(a, [&](const CsrView& t) {
         launch_spmv_t<T, T, T>(t, ph.csr_val, ph.xb.get(),
                                EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
-                                           tune_state, gamma, 0, ph.phase, 0}, st);
+                                           tune_state, hw, gamma, 0, ph.phase, 0}, st);
     }));
     return VAJRA_OK;
 }
@@ -516,6 +523,9 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(cb.part_c.alloc(kCheckBlocks * kQ));
     VJ_TRY(cb.x_last.alloc(n));
     VJ_TRY(cb.y_last.alloc(m));
+    const int K = o.check_frequency > 0 ? o.check_frequency : 64;
+    cb.hw_len = K;
+    VJ_TRY(cb.hw.alloc(2 * static_cast<size_t>(K)));
 
     HState init{};
     const double eta = (o.step_safety > 0.0 && o.step_safety < 1.0 ? o.step_safety : 0.99) / spectral_norm;
@@ -523,6 +533,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     init.eta = eta;
     init.tau = eta / init.omega;
     init.sigma = eta * init.omega;
+    init.inv_sigma = 1.0 / init.sigma;
     init.kkt_start = -1.0;
     init.kkt_prev = -1.0;
     init.bnorm = hn[0];
@@ -537,6 +548,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // FP32 phase, (a64, at64) for the FP64 iterations; every FP64 check uses (a64, at64) too.
     // A handle keeps its first tuning.
     const double gamma = o.reflection;
+    const double gamma32 = (o.mixed_reflection > 0.0 && o.mixed_reflection <= 1.0) ? o.mixed_reflection : gamma;
     CsrView a64 = p.a, at64 = p.at;
     CsrView a32 = p.a, at32 = p.at;
     // Below ~1M entries a solve is launch-bound and the timing runs would cost more than any
@@ -548,7 +560,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             tune.phase = 0;
             VJ_CUDA(cudaMemcpyAsync(dstate.get(), &tune, sizeof(tune), cudaMemcpyHostToDevice, st));
             init_iterates(p32, p, cb, st);
-            VJ_TRY(autotune_iteration<float>(p32, a32, at32, dstate.get(), gamma, st));
+            VJ_TRY(autotune_iteration<float>(p32, a32, at32, dstate.get(), cb, gamma, st));
             h->tuned_a32 = a32.group;
             h->tuned_at32 = at32.group;
             h->tuned |= 1;
@@ -557,7 +569,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             tune.phase = 1;
             VJ_CUDA(cudaMemcpyAsync(dstate.get(), &tune, sizeof(tune), cudaMemcpyHostToDevice, st));
             init_iterates(p64, p, cb, st);
-            VJ_TRY(autotune_iteration<double>(p64, a64, at64, dstate.get(), gamma, st));
+            VJ_TRY(autotune_iteration<double>(p64, a64, at64, dstate.get(), cb, gamma, st));
             h->tuned_a64 = a64.group;
             h->tuned_at64 = at64.group;
             h->tuned |= 2;
@@ -585,6 +597,9 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     else init_iterates(p64, p, cb, st);
     VJ_LAUNCH_CHECK();
     VJ_CUDA(cudaMemcpyAsync(dstate.get(), &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_halpern_weights<<<1, kThreads, 0, st>>>(dstate.get(), cb.hw_len, cb.hw.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
     VJ_CUDA(cudaStreamSynchronize(st));
     const double setup_time = seconds_since(t_start);
 
@@ -603,7 +618,6 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.mixed = mixed ? 1 : 0;
     cp.metric = o.restart_metric == 1 ? 1 : 0;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
-    const int K = o.check_frequency > 0 ? o.check_frequency : 64;
     const int64_t max_iter = o.iteration_limit;
 
     const auto t_iter = Clock::now();
@@ -620,7 +634,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 if (!ph.exec) {
                     const int64_t before = launch_count();
                     VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                    enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, gamma, len, cp, true, st);
+                    enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, ph.phase == 0 ? gamma32 : gamma, len, cp, true, st);
                     VJ_CUDA(cudaStreamEndCapture(st, &ph.graph));
                     VJ_CUDA(cudaGraphInstantiate(&ph.exec, ph.graph, 0));
                     ph.graph_kernels = launch_count() - before;
@@ -629,7 +643,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 VJ_CUDA(cudaGraphLaunch(ph.exec, st));
                 note_launch(ph.graph_kernels);
             } else {
-                enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, gamma, len, cp, false, st);
+                enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, ph.phase == 0 ? gamma32 : gamma, len, cp, false, st);
                 VJ_LAUNCH_CHECK();
             }
             return VAJRA_OK;

@@ -6,10 +6,11 @@
 
 namespace vajra {
 
-constexpr int kHist = 16;
+constexpr int kHist = 32;
 
 struct HState {
     double omega, eta, tau, sigma;
+    double inv_sigma;   // 1 / sigma, kept with sigma so the dual prox multiplies
     double kkt_start, kkt_prev;
     double rel_p, rel_d, rel_gap, rel_kkt, pobj, dobj;
     double bnorm, cnorm, offset_min;
@@ -43,13 +44,15 @@ struct EpiHPrimal {
     const T* c; const T* cl; const T* cu; const T* x0;
     T* x; T* xb; T* xc; T* xprev;
     const HState* st;
+    const double* hw;   // Halpern weights of this chunk: hw[2kk] = (k+1)/(k+2), hw[2kk+1] = 1/(k+2)
     double gamma;
     int kk, phase, write_cand;
-    struct Pre { T xo, c, cl, cu, x0, tau; double k; };
+    struct Pre { T xo, c, cl, cu, x0, tau, w1, w0; };
     __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
     __device__ Pre pre(int j) const {
         Pre p;
-        p.k = static_cast<double>(__ldg(&st->k_base) + kk);
+        p.w1 = static_cast<T>(__ldg(hw + 2 * kk));
+        p.w0 = static_cast<T>(__ldg(hw + 2 * kk + 1));
         p.tau = static_cast<T>(__ldg(&st->tau));
         p.xo = x[j];
         p.c = __ldg(c + j);
@@ -60,13 +63,11 @@ struct EpiHPrimal {
     }
     template <typename Acc>
     __device__ void operator()(int j, Acc v, const Pre& p) const {
-        const T w1 = static_cast<T>((p.k + 1.0) / (p.k + 2.0));
-        const T w0 = static_cast<T>(1.0 / (p.k + 2.0));
         const T g = static_cast<T>(gamma);
         T xp = p.xo - p.tau * (p.c + static_cast<T>(v));
         xp = xp < p.cl ? p.cl : (xp > p.cu ? p.cu : xp);
         xb[j] = xp + xp - p.xo;
-        x[j] = w1 * ((T(1) + g) * xp - g * p.xo) + w0 * p.x0;
+        x[j] = p.w1 * ((T(1) + g) * xp - g * p.xo) + p.w0 * p.x0;
         if (write_cand) { xc[j] = xp; xprev[j] = p.xo; }
     }
     template <typename Acc>
@@ -78,14 +79,17 @@ struct EpiHDual {
     const T* rl; const T* ru; const T* y0;
     T* y; T* yc; T* yprev;
     const HState* st;
+    const double* hw;   // Halpern weights of this chunk (as in EpiHPrimal)
     double gamma;
     int kk, phase, write_cand;
-    struct Pre { T yo, rl, ru, y0, sigma; double k; };
+    struct Pre { T yo, rl, ru, y0, sigma, inv_sigma, w1, w0; };
     __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
     __device__ Pre pre(int i) const {
         Pre p;
-        p.k = static_cast<double>(__ldg(&st->k_base) + kk);
+        p.w1 = static_cast<T>(__ldg(hw + 2 * kk));
+        p.w0 = static_cast<T>(__ldg(hw + 2 * kk + 1));
         p.sigma = static_cast<T>(__ldg(&st->sigma));
+        p.inv_sigma = static_cast<T>(__ldg(&st->inv_sigma));
         p.yo = y[i];
         p.rl = __ldg(rl + i);
         p.ru = __ldg(ru + i);
@@ -94,19 +98,31 @@ struct EpiHDual {
     }
     template <typename Acc>
     __device__ void operator()(int i, Acc w, const Pre& p) const {
-        const T w1 = static_cast<T>((p.k + 1.0) / (p.k + 2.0));
-        const T w0 = static_cast<T>(1.0 / (p.k + 2.0));
         const T g = static_cast<T>(gamma);
         const T yh = p.yo + p.sigma * static_cast<T>(w);
-        T q = yh / p.sigma;
+        T q = yh * p.inv_sigma;
         q = q < p.rl ? p.rl : (q > p.ru ? p.ru : q);
         const T yp = yh - p.sigma * q;
-        y[i] = w1 * ((T(1) + g) * yp - g * p.yo) + w0 * p.y0;
+        y[i] = p.w1 * ((T(1) + g) * yp - g * p.yo) + p.w0 * p.y0;
         if (write_cand) { yc[i] = yp; yprev[i] = p.yo; }
     }
     template <typename Acc>
     __device__ void operator()(int i, Acc w) const { (*this)(i, w, pre(i)); }
 };
+
+// The Halpern weights of the next chunk from the current inner counter: one thread per step.
+__device__ __forceinline__ void halpern_weights(const HState* st, int len, double* hw, int t, int stride) {
+    const long long kb = st->k_base;
+    for (int kk = t; kk < len; kk += stride) {
+        const double k = static_cast<double>(kb + kk);
+        hw[2 * kk] = (k + 1.0) / (k + 2.0);
+        hw[2 * kk + 1] = 1.0 / (k + 2.0);
+    }
+}
+
+__global__ void k_halpern_weights(const HState* st, int len, double* hw) {
+    halpern_weights(st, len, hw, threadIdx.x, blockDim.x);
+}
 
 struct EpiStoreActive {
     double* out;

@@ -22,6 +22,15 @@ import numpy as np
 INF = 1e20
 
 
+def bound_norm(lp) -> float:
+    """||b||_2 of the relative KKT: every finite row bound, an equality row once."""
+    rl, ru = np.asarray(lp.row_lower, float), np.asarray(lp.row_upper, float)
+    rlf, ruf = rl > -INF, ru < INF
+    eq = rlf & ruf & (rl == ru)
+    b2 = np.where(eq, rl ** 2, np.where(rlf, rl, 0.0) ** 2 + np.where(ruf, ru, 0.0) ** 2)
+    return float(np.sqrt(b2.sum()))
+
+
 def relative_kkt(lp, x, row_dual) -> dict:
     A = lp.to_scipy_csc()
     is_max = int(getattr(lp, "sense", 0)) != 0
@@ -43,9 +52,7 @@ def relative_kkt(lp, x, row_dual) -> dict:
     dobj += np.sum(np.where((y < 0) & ruf, y * np.where(ruf, ru, 0.0), 0.0))
     dobj += np.sum(np.where(lam > 0, lam * np.where(lf, cl, 0.0), lam * np.where(uf, cu, 0.0))) + off
     pobj = float(c @ x) + off
-    eq = rlf & ruf & (rl == ru)
-    b2 = np.where(eq, rl ** 2, np.where(rlf, rl, 0.0) ** 2 + np.where(ruf, ru, 0.0) ** 2)
-    rel_p = float(np.linalg.norm(rp) / (1.0 + np.sqrt(b2.sum())))
+    rel_p = float(np.linalg.norm(rp) / (1.0 + bound_norm(lp)))
     rel_d = float(np.linalg.norm(rd) / (1.0 + np.linalg.norm(np.asarray(lp.c, float))))
     rel_gap = float(abs(pobj - dobj) / (1.0 + abs(pobj) + abs(dobj)))
     return {"rel_primal": rel_p, "rel_dual": rel_d, "rel_gap": rel_gap, "rel_kkt": max(rel_p, rel_d, rel_gap),
