@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--clock-period-ms", type=int, default=1000, help="nvidia-smi sampling period in the timed region")
     ap.add_argument("--profile-iters", type=int, default=0,
                     help="profiling aid: one solve capped at this many iterations, then exit (for ncu)")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed")
@@ -274,14 +275,17 @@ def load_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples (every 200 ms) during the timed region."""
+    """nvidia-smi clock / throttle-reason samples during the timed region (every `period_ms`;
+    each query takes driver locks that a solve's per-chunk host synchronisation also needs,
+    so sampling every 200 ms slows a 30 000-iteration solve measurably)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, period_ms: int = 1000):
         self.dev = device_index
+        self.period_ms = period_ms
         self.proc = None
         self.path = None
 
@@ -290,7 +294,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (FileNotFoundError, OSError):
             self.proc = None
@@ -460,7 +464,7 @@ def main():
         solver.run()
     barrier()
     results = []
-    with ClockSampler(local) as clocks:
+    with ClockSampler(local, args.clock_period_ms) as clocks:
         barrier()
         for _ in range(args.steps):
             results.append(solver.run())

@@ -261,10 +261,12 @@ __global__ void k_to_t(int64_t n, const double* __restrict__ s, T* __restrict__ 
 
 // ||b|| (finite row bounds, each equality row once), ||c||, scaled ||b||, ||c|| for the
 // initial primal weight.
-__global__ void __launch_bounds__(1024)
-k_norms(int m, int n, const double* __restrict__ rl_o, const double* __restrict__ ru_o, const double* __restrict__ c_o,
-        const double* __restrict__ rl_s, const double* __restrict__ ru_s, const double* __restrict__ c_s,
-        double* __restrict__ out) {
+// ||b|| (every finite row bound, an equality row once) and ||c||, original and scaled:
+// block partials over a fixed grid, then one CTA adds them in block order (deterministic).
+__global__ void __launch_bounds__(kThreads)
+k_norms_part(int m, int n, const double* __restrict__ rl_o, const double* __restrict__ ru_o,
+             const double* __restrict__ c_o, const double* __restrict__ rl_s, const double* __restrict__ ru_s,
+             const double* __restrict__ c_s, double* __restrict__ part) {
     __shared__ double red[4 * 32];
     double v[4] = {0, 0, 0, 0};
     auto b2 = [](double l, double u) {
@@ -272,8 +274,25 @@ k_norms(int m, int n, const double* __restrict__ rl_o, const double* __restrict_
         if (lf && uf && l == u) return l * l;
         return (lf ? l * l : 0.0) + (uf ? u * u : 0.0);
     };
-    for (int i = threadIdx.x; i < m; i += blockDim.x) { v[0] += b2(rl_o[i], ru_o[i]); v[2] += b2(rl_s[i], ru_s[i]); }
-    for (int j = threadIdx.x; j < n; j += blockDim.x) { v[1] += c_o[j] * c_o[j]; v[3] += c_s[j] * c_s[j]; }
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        v[0] += b2(rl_o[i], ru_o[i]);
+        v[2] += b2(rl_s[i], ru_s[i]);
+    }
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        v[1] += c_o[j] * c_o[j];
+        v[3] += c_s[j] * c_s[j];
+    }
+    block_reduce<OpSum, double, 4>(v, red);
+    if (threadIdx.x == 0) for (int q = 0; q < 4; ++q) part[blockIdx.x * 4 + q] = v[q];
+}
+
+__global__ void __launch_bounds__(1024)
+k_norms_final(int nb, const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double red[4 * 32];
+    double v[4] = {0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+        for (int q = 0; q < 4; ++q) v[q] += part[b * 4 + q];
     block_reduce<OpSum, double, 4>(v, red);
     if (threadIdx.x == 0) for (int q = 0; q < 4; ++q) out[q] = sqrt(v[q]);
 }
@@ -297,11 +316,21 @@ __global__ void k_widen(int k, const T* __restrict__ s, double* __restrict__ d) 
     if (i < k) d[i] = static_cast<double>(s[i]);
 }
 
-__global__ void __launch_bounds__(1024)
-k_dot_offset(int n, const double* __restrict__ a, const double* __restrict__ b, double offset, double* out) {
+// offset + a.b, in the same two deterministic stages.
+__global__ void __launch_bounds__(kThreads)
+k_dot_part(int n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part) {
     __shared__ double red[32];
     double v[1] = {0.0};
-    for (int j = threadIdx.x; j < n; j += blockDim.x) v[0] += a[j] * b[j];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) v[0] += a[j] * b[j];
+    block_reduce<OpSum, double, 1>(v, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+__global__ void __launch_bounds__(1024)
+k_dot_final(int nb, const double* __restrict__ part, double offset, double* __restrict__ out) {
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v[0] += part[b];
     block_reduce<OpSum, double, 1>(v, red);
     if (threadIdx.x == 0) *out = offset + v[0];
 }
@@ -495,10 +524,13 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // Norms for the relative KKT and the initial primal weight.
     DeviceBuffer<double> norms;
     VJ_TRY(norms.alloc(4));
-    k_norms<<<1, 1024, 0, st>>>(m, n, lp.row_lower.get(), lp.row_upper.get(), lp.c.get(), p.row_lower.get(),
-                               p.row_upper.get(), p.c.get(), norms.get());
+    DeviceBuffer<double> red_part;
+    VJ_TRY(red_part.alloc(4 * static_cast<size_t>(kCheckBlocks)));
+    k_norms_part<<<kCheckBlocks, kThreads, 0, st>>>(m, n, lp.row_lower.get(), lp.row_upper.get(), lp.c.get(),
+                                                   p.row_lower.get(), p.row_upper.get(), p.c.get(), red_part.get());
+    k_norms_final<<<1, 1024, 0, st>>>(kCheckBlocks, red_part.get(), norms.get());
     VJ_LAUNCH_CHECK();
-    note_launch(1);
+    note_launch(2);
     double hn[4];
     VJ_CUDA(cudaMemcpyAsync(hn, norms.get(), sizeof(hn), cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaStreamSynchronize(st));
@@ -708,9 +740,10 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     launch_spmv_t<double, double, double>(a64, p.csr_val_orig.get(), x_out.get(), EpiStore<double>{row_value.get()}, st);
     launch_spmv_t<double, double, double>(at64, lp.values.get(), y_out.get(), EpiStore<double>{col_dual.get()}, st);
     k_reduced_costs<<<grid_for(n), kThreads, 0, st>>>(n, lp.c.get(), is_max ? 1 : 0, col_dual.get());
-    k_dot_offset<<<1, 1024, 0, st>>>(n, lp.c.get(), x_out.get(), h->objective_offset, obj.get());
+    k_dot_part<<<kCheckBlocks, kThreads, 0, st>>>(n, lp.c.get(), x_out.get(), cb.part_r.get());
+    k_dot_final<<<1, 1024, 0, st>>>(kCheckBlocks, cb.part_r.get(), h->objective_offset, obj.get());
     VJ_LAUNCH_CHECK();
-    note_launch(cur_phase == 0 ? 5 : 3);
+    note_launch(cur_phase == 0 ? 6 : 4);
     double objective = 0.0;
     VJ_CUDA(cudaMemcpyAsync(&objective, obj.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaMemcpyAsync(hs, S, sizeof(HState), cudaMemcpyDeviceToHost, st));
