@@ -115,6 +115,18 @@ def test_reference_test_lps_reach_optimum(cuda, prec, case):
     check_solution(lp, g, obj=opt)
 
 
+@pytest.mark.parametrize("shape", [-1, -2, 1, 2, 4, 8, 16, 32])
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_every_spmv_shape_reaches_the_optimum(cuda, prec, shape):
+    """Each launch shape of the iteration kernels (row blocks with one or two load groups,
+    1..32 lanes per row), forced for both SpMVs, solves to the tolerance."""
+    lp = W.random_planted(600, 1500, (2, 40), seed=31)
+    g = V.solve(lp, precision=prec, spmv_shape_a=shape, spmv_shape_at=shape)
+    want = 0 if shape == -1 else (64 if shape == -2 else shape)
+    assert g["spmv_group_a"] == want and g["spmv_group_at"] == want
+    check_solution(lp, g, obj=lp.planted_objective)
+
+
 @pytest.mark.parametrize("prec", PRECISIONS)
 def test_deterministic(cuda, prec):
     lp = W.random_planted(500, 1200, 6, seed=21)

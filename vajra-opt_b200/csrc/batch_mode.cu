@@ -183,7 +183,7 @@ struct BlockList {
         inst = inst_;
         rows = v.rows;
         int cap;
-        if (v.group == 0 && v.block_rows) {
+        if (is_rowblock_shape(v.group) && v.block_rows) {
             nblocks = v.nb;
             block_rows = v.block_rows;
             cap = sms * 4;
@@ -613,7 +613,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
             const double* val = (v == &a) ? p.csr_val.get() : p.csc_val.get();
             float best = 1e30f;
             int best_g = v->group;
-            for (int g : {0, 1, 2, 4, 8, 16, 32}) {
+            for (int g : {0, kRowblock2, 1, 2, 4, 8, 16, 32}) {
                 CsrView t = *v;
                 t.group = g;
                 launch_spmv_t<double, double, double>(t, val, xin, EpiStorePlain{out}, st);

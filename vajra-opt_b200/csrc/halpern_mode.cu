@@ -430,7 +430,8 @@ void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrV
     enqueue_check(ph, a64, at64, p, lp, cb, S, cp, st);
 }
 
-// Times every launch shape (row-block kernel, 1..32 lanes per row) of both iteration kernels
+// Times every launch shape (row-block kernel with one or two load groups, 1..32 lanes per
+// row) of both iteration kernels
 // with their real epilogues and keeps the fastest per matrix.  `tune_state` is a scratch
 // state whose phase is the tuned one; the iterates it scribbles on are re-initialised after.
 template <typename T>
@@ -447,7 +448,7 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
         if (v.rows <= 0) return VAJRA_OK;
         float best = 1e30f;
         int best_g = v.group;
-        for (int g : {0, 1, 2, 4, 8, 16, 32}) {
+        for (int g : {0, kRowblock2, 1, 2, 4, 8, 16, 32}) {
             CsrView t = v;
             t.group = g;
             launch(t);   // warm
@@ -616,8 +617,9 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         at64.group = h->tuned_at64;
     }
     auto forced = [](int32_t shape, CsrView& v32, CsrView& v64) {   // caller-fixed shapes
-        if (shape == -1 || shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16 || shape == 32)
-            v32.group = v64.group = shape == -1 ? 0 : shape;
+        if (shape == -1 || shape == -2 || shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16 ||
+            shape == 32)
+            v32.group = v64.group = shape == -1 ? 0 : (shape == -2 ? kRowblock2 : shape);
     };
     forced(o.spmv_shape_a, a32, a64);
     forced(o.spmv_shape_at, at32, at64);

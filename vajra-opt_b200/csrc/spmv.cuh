@@ -220,7 +220,8 @@ template <typename VV>
 constexpr int rowblock_min_blocks() { return sizeof(VV) == 4 ? 6 : 4; }
 
 // One row block (tile b).  Every exit before the first barrier is uniform over the CTA.
-template <typename VV, typename VX, typename Acc, class Epi>
+// U: groups of four entries a thread loads before it gathers (all U groups' loads in flight).
+template <typename VV, typename VX, typename Acc, int U, class Epi>
 __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                               const VV* __restrict__ val, const VX* __restrict__ x,
                                               const TileDesc* __restrict__ tiles, Acc* prod, int* med_rows,
@@ -239,21 +240,33 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
         my_s = static_cast<int>(ptr[my_row] - e0);
         my_e = static_cast<int>(ptr[my_row + 1] - e0);
     }
-    for (int64_t q = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x); q < e1; q += 4 * blockDim.x) {
-        int ii[4];
-        VV vv[4];
-        load4(idx + q, ii);
-        load4(val + q, vv);
-        Acc pr[4];
+    const int64_t qstride = 4 * static_cast<int64_t>(blockDim.x);
+    for (int64_t q0 = (e0 & ~int64_t(3)) + 4 * static_cast<int64_t>(threadIdx.x); q0 < e1; q0 += U * qstride) {
+        int ii[U][4];
+        VV vv[U][4];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int64_t k = q + t;
-            pr[t] = (k >= e0 && k < e1) ? static_cast<Acc>(vv[t]) * static_cast<Acc>(ld_cached(x + ii[t])) : Acc(0);
+        for (int u = 0; u < U; ++u) {
+            const int64_t q = q0 + u * qstride;
+            if (q < e1) {
+                load4(idx + q, ii[u]);
+                load4(val + q, vv[u]);
+            }
         }
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const int64_t k = q + t;
-            if (k >= e0 && k < e1) prod[k - e0] = pr[t];
+        for (int u = 0; u < U; ++u) {
+            const int64_t q = q0 + u * qstride;
+            Acc pr[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int64_t k = q + t;
+                pr[t] = (k >= e0 && k < e1) ? static_cast<Acc>(vv[u][t]) * static_cast<Acc>(ld_cached(x + ii[u][t]))
+                                            : Acc(0);
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int64_t k = q + t;
+                if (k >= e0 && k < e1) prod[k - e0] = pr[t];
+            }
         }
     }
     if (threadIdx.x == 0) n_med = 0;
@@ -285,8 +298,8 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
 // CTAs [0, nb) take row blocks: block blockIdx.x, or -- in list mode (blk_list != null) --
 // blocks blk_list[t] for t = blockIdx.x, + nb, ... < *blk_count.  CTAs from nb on take one
 // row longer than kTile each.
-template <typename VV, typename VX, typename Acc, class Epi>
-__global__ void __launch_bounds__(kThreads, rowblock_min_blocks<VV>())
+template <typename VV, typename VX, typename Acc, class Epi, int MB = rowblock_min_blocks<VV>(), int U = 1>
+__global__ void __launch_bounds__(kThreads, MB)
 k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const VV* __restrict__ val,
                 const VX* __restrict__ x, const TileDesc* __restrict__ tiles, int nb,
                 const int32_t* __restrict__ long_rows, const int32_t* __restrict__ blk_list,
@@ -310,12 +323,12 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
         return;
     }
     if (blk_list == nullptr) {
-        rowblock_tile<VV, VX, Acc>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        rowblock_tile<VV, VX, Acc, U>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
         return;
     }
     const int cnt = *blk_count;
     for (int t = blockIdx.x; t < cnt; t += nb) {
-        rowblock_tile<VV, VX, Acc>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        rowblock_tile<VV, VX, Acc, U>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
         __syncthreads();   // the tile's shared state is reused by the next one
     }
 }
@@ -328,7 +341,7 @@ struct CsrView {
     int64_t nnz = 0;
     const int64_t* ptr = nullptr;
     const int32_t* idx = nullptr;
-    int group = 8;                      // lanes per row (1,2,4,...,32); 0 = row-block kernel
+    int group = 8;                      // lanes per row (1,2,4,...,32); 0 / kRowblock2 = row-block kernel
     int64_t long_len = 1 << 30;         // grouped-lane kernel: rows longer than this go one CTA per row
     const int32_t* long_rows = nullptr; // device list of those rows
     int n_long = 0;
@@ -344,11 +357,17 @@ struct CsrView {
     int blk_grid = 0;
 };
 
-template <typename VV, typename VX, typename Acc, class Epi>
+// Launch-shape code of the row-block kernel with two groups of four entries in flight per
+// thread (U = 2; one resident CTA less per SM with 4-byte values).  Group 0 is U = 1.
+constexpr int kRowblock2 = 64;
+inline bool is_rowblock_shape(int group) { return group == 0 || group == kRowblock2; }
+
+template <typename VV, typename VX, typename Acc, int U = 1, class Epi>
 inline void launch_rowblock(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     const size_t smem = sizeof(Acc) * 2 * kTile;
     const int nb = a.blk_list ? a.blk_grid : a.nb;
-    k_spmv_rowblock<VV, VX, Acc, Epi><<<nb + a.rb_n_long, kThreads, smem, st>>>(
+    constexpr int MB = U == 1 ? rowblock_min_blocks<VV>() : (sizeof(VV) == 4 ? 5 : 4);
+    k_spmv_rowblock<VV, VX, Acc, Epi, MB, U><<<nb + a.rb_n_long, kThreads, smem, st>>>(
         a.ptr, a.idx, val, x, a.tiles, nb, a.rb_long_rows, a.blk_list, a.blk_count, epi);
     note_launch();
 }
@@ -364,13 +383,17 @@ inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, 
     note_launch();
 }
 
-// group 0 selects the row-block kernel; other lane-group sizes than 1..16 dispatch to 32.
+// group 0 / kRowblock2 select the row-block kernel; other lane-group sizes than 1..16 dispatch to 32.
 template <typename VV, typename VX, typename Acc, class Epi>
 inline void launch_spmv_t(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     if (a.rows <= 0) return;
     switch (a.group) {
         case 0:
-            if (a.tiles) { launch_rowblock<VV, VX, Acc>(a, val, x, epi, st); break; }
+            if (a.tiles) { launch_rowblock<VV, VX, Acc, 1>(a, val, x, epi, st); break; }
+            launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st);
+            break;
+        case kRowblock2:
+            if (a.tiles) { launch_rowblock<VV, VX, Acc, 2>(a, val, x, epi, st); break; }
             launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st);
             break;
         case 1: launch_vec_g<VV, VX, Acc, 1>(a, val, x, epi, st); break;
