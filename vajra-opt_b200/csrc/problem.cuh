@@ -98,4 +98,10 @@ vajra_status spectral_norm_fast(const Prepared& p, int m, int n, int max_iter, d
 // may override `group`).
 vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st);
 
+// Row-block partition of `v` at `tile` entries per block: nb + 1 block boundaries, the nb
+// block descriptors, and the rows longer than `tile` (one CTA each).
+vajra_status build_row_partition(const CsrView& v, int64_t tile, DeviceBuffer<int32_t>& blocks,
+                                 DeviceBuffer<TileDesc>& tiles, DeviceBuffer<int32_t>& long_rows, int* nb,
+                                 int* n_long, cudaStream_t st);
+
 }  // namespace vajra

@@ -494,12 +494,12 @@ __global__ void k_rowblock_partition(int rows, const int64_t* __restrict__ ptr, 
 }
 
 __global__ void k_tile_desc(int nb, const int64_t* __restrict__ ptr, const int32_t* __restrict__ block_rows,
-                            TileDesc* __restrict__ tiles) {
+                            int64_t tile, TileDesc* __restrict__ tiles) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     const int r0 = block_rows[b], r1 = block_rows[b + 1];
     int r_end = r1;
-    if (r1 > r0 && ptr[r1] - ptr[r1 - 1] > kTile) r_end = r1 - 1;
+    if (r1 > r0 && ptr[r1] - ptr[r1 - 1] > tile) r_end = r1 - 1;
     TileDesc d;
     d.r0 = r0;
     d.r_end = r_end > r0 ? r_end : r0;
@@ -524,6 +524,24 @@ static vajra_status collect_long(const CsrView& v, int64_t long_len, DeviceBuffe
     return VAJRA_OK;
 }
 
+vajra_status build_row_partition(const CsrView& v, int64_t tile, DeviceBuffer<int32_t>& blocks,
+                                 DeviceBuffer<TileDesc>& tiles, DeviceBuffer<int32_t>& long_rows, int* nb,
+                                 int* n_long, cudaStream_t st) {
+    int64_t nb64 = (v.nnz + tile - 1) / tile;
+    if (nb64 < 1) nb64 = 1;
+    if (nb64 > (1LL << 30)) { set_error("matrix too large for the row-block partition"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    *nb = static_cast<int>(nb64);
+    VJ_TRY(blocks.alloc(static_cast<size_t>(*nb) + 1));
+    k_rowblock_partition<<<grid_for(static_cast<int64_t>(*nb) + 1), kThreads, 0, st>>>(v.rows, v.ptr, tile, *nb,
+                                                                                       blocks.get());
+    VJ_LAUNCH_CHECK();
+    VJ_TRY(tiles.alloc(static_cast<size_t>(*nb)));
+    k_tile_desc<<<grid_for(*nb), kThreads, 0, st>>>(*nb, v.ptr, blocks.get(), tile, tiles.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(2);
+    return collect_long(v, tile, long_rows, n_long, st);
+}
+
 static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, DeviceBuffer<int32_t>& blocks,
                              DeviceBuffer<TileDesc>& tiles, DeviceBuffer<int32_t>& rb_list, cudaStream_t st) {
     const double mean = v.rows > 0 ? static_cast<double>(v.nnz) / v.rows : 0.0;
@@ -533,23 +551,9 @@ static vajra_status plan_one(CsrView& v, DeviceBuffer<int32_t>& list, DeviceBuff
     v.long_len = long_len;
     VJ_TRY(collect_long(v, long_len, list, &v.n_long, st));
     v.long_rows = list.get();
-    // row-block partition
-    int64_t nb64 = (v.nnz + kTile - 1) / kTile;
-    if (nb64 < 1) nb64 = 1;
-    if (nb64 > (1LL << 30)) { set_error("matrix too large for the row-block partition"); return VAJRA_ERR_INVALID_ARGUMENT; }
-    v.nb = static_cast<int>(nb64);
-    VJ_TRY(blocks.alloc(static_cast<size_t>(v.nb) + 1));
-    k_rowblock_partition<<<grid_for(static_cast<int64_t>(v.nb) + 1), kThreads, 0, st>>>(v.rows, v.ptr, kTile, v.nb,
-                                                                                        blocks.get());
-    VJ_LAUNCH_CHECK();
-    note_launch(1);
+    VJ_TRY(build_row_partition(v, kTile, blocks, tiles, rb_list, &v.nb, &v.rb_n_long, st));
     v.block_rows = blocks.get();
-    VJ_TRY(tiles.alloc(static_cast<size_t>(v.nb)));
-    k_tile_desc<<<grid_for(v.nb), kThreads, 0, st>>>(v.nb, v.ptr, v.block_rows, tiles.get());
-    VJ_LAUNCH_CHECK();
-    note_launch(1);
     v.tiles = tiles.get();
-    VJ_TRY(collect_long(v, kTile, rb_list, &v.rb_n_long, st));
     v.rb_long_rows = rb_list.get();
     return VAJRA_OK;
 }

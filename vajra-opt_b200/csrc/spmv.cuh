@@ -221,7 +221,7 @@ constexpr int rowblock_min_blocks() { return sizeof(VV) == 4 ? 6 : 4; }
 
 // One row block (tile b).  Every exit before the first barrier is uniform over the CTA.
 // U: groups of four entries a thread loads before it gathers (all U groups' loads in flight).
-template <typename VV, typename VX, typename Acc, int U, class Epi>
+template <typename VV, typename VX, typename Acc, int U, int KT, int MR, class Epi>
 __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                               const VV* __restrict__ val, const VX* __restrict__ x,
                                               const TileDesc* __restrict__ tiles, Acc* prod, int* med_rows,
@@ -274,7 +274,7 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
     for (int r = my_row; r < r_end; r += blockDim.x) {
         const int s = r == my_row ? my_s : static_cast<int>(ptr[r] - e0);
         const int e = r == my_row ? my_e : static_cast<int>(ptr[r + 1] - e0);
-        if (e - s > kMediumRow) {
+        if (e - s > MR) {
             med_rows[atomicAdd(&n_med, 1)] = r;
             continue;
         }
@@ -298,7 +298,8 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
 // CTAs [0, nb) take row blocks: block blockIdx.x, or -- in list mode (blk_list != null) --
 // blocks blk_list[t] for t = blockIdx.x, + nb, ... < *blk_count.  CTAs from nb on take one
 // row longer than kTile each.
-template <typename VV, typename VX, typename Acc, class Epi, int MB = rowblock_min_blocks<VV>(), int U = 1>
+template <typename VV, typename VX, typename Acc, class Epi, int MB = rowblock_min_blocks<VV>(), int U = 1,
+          int KT = kTile, int MR = kMediumRow>
 __global__ void __launch_bounds__(kThreads, MB)
 k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const VV* __restrict__ val,
                 const VX* __restrict__ x, const TileDesc* __restrict__ tiles, int nb,
@@ -306,7 +307,7 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
                 const int* __restrict__ blk_count, Epi epi) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Acc* prod = reinterpret_cast<Acc*>(smem_raw);
-    __shared__ int med_rows[kMaxMediumRows];
+    __shared__ int med_rows[(2 * KT) / MR + 1];
     __shared__ int n_med;
     __shared__ Acc red[32];
     if (!epi.active()) return;
@@ -323,12 +324,12 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
         return;
     }
     if (blk_list == nullptr) {
-        rowblock_tile<VV, VX, Acc, U>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        rowblock_tile<VV, VX, Acc, U, KT, MR>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
         return;
     }
     const int cnt = *blk_count;
     for (int t = blockIdx.x; t < cnt; t += nb) {
-        rowblock_tile<VV, VX, Acc, U>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        rowblock_tile<VV, VX, Acc, U, KT, MR>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
         __syncthreads();   // the tile's shared state is reused by the next one
     }
 }
