@@ -190,7 +190,6 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
 // trailing CTAs of the same launch.  A block's staged entries never exceed 2 kTile - 1.
 constexpr int kTile = 2048;
 constexpr int kMediumRow = 48;
-constexpr int kMaxMediumRows = (2 * kTile) / kMediumRow + 1;
 
 __device__ __forceinline__ void load4(const int32_t* p, int (&v)[4]) {
     const int4 t = __ldcs(reinterpret_cast<const int4*>(p));
