@@ -156,3 +156,59 @@ def test_mixed_splits_iterations(cuda):
     lp = W.random_planted(2000, 5000, 8, seed=24)
     g = V.solve(lp, precision=V.PREC_MIXED)
     assert g["fp32_iterations"] > 0 and g["fp32_iterations"] + g["fp64_iterations"] == g["iterations"]
+
+
+def with_structure(lp, dense_row=None, dense_col=None, empty_rows=(), empty_cols=(), seed=0):
+    """lp with one dense row / column added to A and some rows / columns emptied (their bounds
+    kept satisfiable), rebuilt through the canonical CSC of the generators."""
+    rng = np.random.default_rng(seed)
+    A = lp.to_scipy_csc().tocoo()
+    keep = ~np.isin(A.row, list(empty_rows)) & ~np.isin(A.col, list(empty_cols))
+    r, c, v = list(A.row[keep]), list(A.col[keep]), list(A.data[keep])
+    if dense_row is not None:
+        cols = np.setdiff1d(np.arange(lp.num_cols), list(empty_cols))
+        r += [dense_row] * len(cols); c += list(cols); v += list(rng.uniform(-1e-3, 1e-3, len(cols)))
+    if dense_col is not None:
+        rows = np.setdiff1d(np.arange(lp.num_rows), list(empty_rows))
+        r += list(rows); c += [dense_col] * len(rows); v += list(rng.uniform(-1e-3, 1e-3, len(rows)))
+    cp, ri, vals = W.canonical_csc(lp.num_rows, lp.num_cols, np.array(r), np.array(c), np.array(v))
+    out = W.LP(lp.num_rows, lp.num_cols, cp, ri, vals, lp.c.copy(), lp.col_lower.copy(), lp.col_upper.copy(),
+               lp.row_lower.copy(), lp.row_upper.copy(), sense=lp.sense)
+    x = np.clip(np.zeros(lp.num_cols), out.col_lower, out.col_upper)
+    ax = out.to_scipy_csc() @ x
+    # feasible by construction: every row range holds A x0 for the bound-clipped x0 = 0 point
+    out.row_lower = np.where(out.row_lower > -INF, np.minimum(out.row_lower, ax - 1.0), out.row_lower)
+    out.row_upper = np.where(out.row_upper < INF, np.maximum(out.row_upper, ax + 1.0), out.row_upper)
+    for i in empty_rows:
+        out.row_lower[i], out.row_upper[i] = -1.0, 1.0
+    return out
+
+
+@pytest.mark.parametrize("shape", [-1, -2, 4, 32])
+def test_long_rows_and_empty_rows_and_columns(cuda, shape):
+    """A row and a column longer than a row block (2048 entries: the one-CTA-per-row paths of
+    both kernels) plus empty rows and columns, under the fixed launch shapes."""
+    base = W.small_random(2600, 3000, 12)
+    lp = with_structure(base, dense_row=7, dense_col=11, empty_rows=(3, 50, 2599), empty_cols=(0, 99, 2999), seed=1)
+    nnz = np.diff(lp.col_ptr)
+    assert nnz.max() > 2048 and (nnz == 0).sum() >= 3
+    g = V.solve(lp, precision=V.PREC_FP64, spmv_shape_a=shape, spmv_shape_at=shape)
+    check_solution(lp, g, obj=highs(lp))
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_infeasible_lp_is_not_reported_optimal(cuda, prec):
+    # x0 + x1 >= 4 and x0 + x1 <= 1 with 0 <= x <= 10
+    cp, ri, vals = W.canonical_csc(2, 2, np.array([0, 0, 1, 1]), np.array([0, 1, 0, 1]), np.ones(4))
+    lp = W.LP(2, 2, cp, ri, vals, np.array([1.0, 1.0]), np.zeros(2), np.full(2, 10.0), np.array([4.0, -INF]),
+              np.array([INF, 1.0]))
+    g = V.solve(lp, precision=prec, iteration_limit=20000)
+    assert g["status_name"] != "OPTIMAL"
+    assert g["rel_kkt"] > 1e-6
+
+
+def test_time_limit_stops_the_solve(cuda):
+    lp = W.random_planted(2000, 5000, 8, seed=5)
+    g = V.solve(lp, precision=V.PREC_FP64, time_limit=1e-4)
+    assert g["status_name"] == "TIME_LIMIT"
+    assert g["iterations"] < 5000
