@@ -220,7 +220,8 @@ constexpr int rowblock_min_blocks() { return sizeof(VV) == 4 ? 6 : 4; }
 
 // One row block (tile b).  Every exit before the first barrier is uniform over the CTA.
 // U: groups of four entries a thread loads before it gathers (all U groups' loads in flight).
-template <typename VV, typename VX, typename Acc, int U, int KT, int MR, class Epi>
+// PRE: issue the epilogue's early loads (two-phase epilogues) for the thread's first row.
+template <typename VV, typename VX, typename Acc, int U, int KT, int MR, bool PRE, class Epi>
 __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                                               const VV* __restrict__ val, const VX* __restrict__ x,
                                               const TileDesc* __restrict__ tiles, Acc* prod, int* med_rows,
@@ -235,7 +236,7 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
     PreOf<Epi> pre{};
     int my_s = 0, my_e = 0;
     if (my_row < r_end) {
-        pre = epi_pre(epi, my_row, 0);
+        if constexpr (PRE) pre = epi_pre(epi, my_row, 0);
         my_s = static_cast<int>(ptr[my_row] - e0);
         my_e = static_cast<int>(ptr[my_row + 1] - e0);
     }
@@ -279,7 +280,7 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
         }
         Acc acc = Acc(0);
         for (int k = s; k < e; ++k) acc += prod[k];
-        if (r == my_row) epi_fin(epi, r, acc, pre, 0);
+        if (PRE && r == my_row) epi_fin(epi, r, acc, pre, 0);
         else epi(r, acc);
     }
     __syncthreads();
@@ -298,7 +299,7 @@ __device__ __forceinline__ void rowblock_tile(int b, const int64_t* __restrict__
 // blocks blk_list[t] for t = blockIdx.x, + nb, ... < *blk_count.  CTAs from nb on take one
 // row longer than kTile each.
 template <typename VV, typename VX, typename Acc, class Epi, int MB = rowblock_min_blocks<VV>(), int U = 1,
-          int KT = kTile, int MR = kMediumRow>
+          int KT = kTile, int MR = kMediumRow, bool PRE = true>
 __global__ void __launch_bounds__(kThreads, MB)
 k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const VV* __restrict__ val,
                 const VX* __restrict__ x, const TileDesc* __restrict__ tiles, int nb,
@@ -323,12 +324,12 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
         return;
     }
     if (blk_list == nullptr) {
-        rowblock_tile<VV, VX, Acc, U, KT, MR>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        rowblock_tile<VV, VX, Acc, U, KT, MR, PRE>(blockIdx.x, ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
         return;
     }
     const int cnt = *blk_count;
     for (int t = blockIdx.x; t < cnt; t += nb) {
-        rowblock_tile<VV, VX, Acc, U, KT, MR>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
+        rowblock_tile<VV, VX, Acc, U, KT, MR, PRE>(blk_list[t], ptr, idx, val, x, tiles, prod, med_rows, n_med, epi);
         __syncthreads();   // the tile's shared state is reused by the next one
     }
 }
@@ -358,7 +359,9 @@ struct CsrView {
 };
 
 // Launch-shape code of the row-block kernel with two groups of four entries in flight per
-// thread (U = 2; one resident CTA less per SM with 4-byte values).  Group 0 is U = 1.
+// thread (U = 2).  With 4-byte values it keeps six CTAs per SM by leaving the epilogue's loads
+// to the end (they would not fit in 40 registers); with 8-byte values it keeps them early at
+// four CTAs per SM.  Group 0 is U = 1 with early epilogue loads.
 constexpr int kRowblock2 = 64;
 inline bool is_rowblock_shape(int group) { return group == 0 || group == kRowblock2; }
 
@@ -366,8 +369,9 @@ template <typename VV, typename VX, typename Acc, int U = 1, class Epi>
 inline void launch_rowblock(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     const size_t smem = sizeof(Acc) * 2 * kTile;
     const int nb = a.blk_list ? a.blk_grid : a.nb;
-    constexpr int MB = U == 1 ? rowblock_min_blocks<VV>() : (sizeof(VV) == 4 ? 5 : 4);
-    k_spmv_rowblock<VV, VX, Acc, Epi, MB, U><<<nb + a.rb_n_long, kThreads, smem, st>>>(
+    constexpr int MB = U == 1 ? rowblock_min_blocks<VV>() : (sizeof(VV) == 4 ? 6 : 4);
+    constexpr bool PRE = U == 1 || sizeof(VV) != 4;
+    k_spmv_rowblock<VV, VX, Acc, Epi, MB, U, kTile, kMediumRow, PRE><<<nb + a.rb_n_long, kThreads, smem, st>>>(
         a.ptr, a.idx, val, x, a.tiles, nb, a.rb_long_rows, a.blk_list, a.blk_count, epi);
     note_launch();
 }
