@@ -386,6 +386,14 @@ def workload_config(args, lp):
 def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
+    try:
+        return run(args, world, rank, local, dist)
+    finally:
+        if dist is not None and dist.is_initialized():
+            dist.destroy_process_group()
+
+
+def run(args, world, rank, local, dist):
     import numpy as np
     from vajra_pdhg import workloads as W
 
@@ -563,7 +571,6 @@ def main():
         print(json.dumps(line))
     if dist:
         dist.barrier()
-        dist.destroy_process_group()
     return 0
 
 

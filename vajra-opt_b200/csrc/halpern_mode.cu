@@ -16,6 +16,9 @@
 // mixed precision -- the hand-over from the FP32 phase to the FP64 polish.
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "halpern_state.cuh"
@@ -485,6 +488,20 @@ void init_iterates(Phase<T>& ph, const Prepared& p, CheckBuffers& cb, cudaStream
     note_launch(1);
 }
 
+// Launch shapes found by the autotuner, shared by every handle of the process whose LP has the
+// same device, dimensions and number of entries (the shapes only change speed, never results),
+// so repeated solves of one LP pay the timing runs once.
+struct TuneKey {
+    int device, m, n;
+    int64_t nnz;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(device, m, n, nnz) < std::tie(o.device, o.m, o.n, o.nnz);
+    }
+};
+struct TuneEntry { int bits = 0, a32 = 8, at32 = 8, a64 = 8, at64 = 8; };
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneEntry> g_tune_cache;
+
 }  // namespace
 
 vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
@@ -587,6 +604,16 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // Below ~1M entries a solve is launch-bound and the timing runs would cost more than any
     // shape saves: the set-up heuristic (lanes per row from the mean row length) stays.
     constexpr int64_t kAutotuneMinNnz = int64_t(1) << 20;
+    const TuneKey tkey{h->device, m, n, nnz};
+    if (o.autotune) {   // shapes another handle already tuned for this LP
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(tkey);
+        if (it != g_tune_cache.end()) {
+            const TuneEntry& e = it->second;
+            if ((e.bits & 1) && !(h->tuned & 1)) { h->tuned_a32 = e.a32; h->tuned_at32 = e.at32; h->tuned |= 1; }
+            if ((e.bits & 2) && !(h->tuned & 2)) { h->tuned_a64 = e.a64; h->tuned_at64 = e.at64; h->tuned |= 2; }
+        }
+    }
     if (o.autotune && nnz >= kAutotuneMinNnz && (!(h->tuned & 2) || (mixed && !(h->tuned & 1)))) {
         HState tune = init;
         if (mixed && !(h->tuned & 1)) {
@@ -607,6 +634,11 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             h->tuned_at64 = at64.group;
             h->tuned |= 2;
         }
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        TuneEntry& e = g_tune_cache[tkey];
+        if (h->tuned & 1) { e.a32 = h->tuned_a32; e.at32 = h->tuned_at32; }
+        if (h->tuned & 2) { e.a64 = h->tuned_a64; e.at64 = h->tuned_at64; }
+        e.bits |= h->tuned;
     }
     if (h->tuned & 1) {
         a32.group = h->tuned_a32;
