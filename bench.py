@@ -57,8 +57,9 @@ def parse():
                     help="profiling aid: one solve capped at this many iterations, then exit (for ncu)")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--shapes", default=None,
-                    help="profiling: fixed SpMV launch shapes 'A,AT' (-1 row block, 1..32 lanes per row) "
-                         "instead of autotuning, whose timings a profiler would distort")
+                    help="profiling: fixed SpMV launch shapes 'A,AT' (-1 row block, -2 row block with two load "
+                         "groups, 1..32 lanes per row; write --shapes=-2,-2) instead of autotuning, whose timings a "
+                         "profiler would distort")
     ap.add_argument("--batch", type=int, default=0,
                     help="batched workload instead: this many config-0-style LPs (m log-uniform on "
                          "[100, 20000]), one batched solve vs the same LPs solved one after another")
