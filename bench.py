@@ -60,6 +60,8 @@ def parse():
                     help="profiling: fixed SpMV launch shapes 'A,AT' (-1 row block, -2 row block with two load "
                          "groups, 1..32 lanes per row; write --shapes=-2,-2) instead of autotuning, whose timings a "
                          "profiler would distort")
+    ap.add_argument("--degree-order", type=int, default=0, choices=[-1, 0, 1],
+                    help="row / column renumbering by entry count: 0 auto (on from 2^20 entries), 1 on, -1 off")
     ap.add_argument("--batch", type=int, default=0,
                     help="batched workload instead: this many config-0-style LPs (m log-uniform on "
                          "[100, 20000]), one batched solve vs the same LPs solved one after another")
@@ -380,6 +382,7 @@ def workload_config(args, lp):
                         f"truncated power law on [2,2000], mean 10; values N(0,1) stored FP32), seed {args.seed}",
             "nnz": int(lp.nnz), "tolerance": "FP64 relative KKT <= 1e-6 on the original LP",
             "precision": "mixed: FP32 iterations + FP64 checks and FP64 polish",
+            "degree_order": {0: "auto (on from 2^20 entries)", 1: "on", -1: "off"}[args.degree_order],
             "l2": "inputs larger than L2 (A alone is ~240 MB in FP64 CSC), no flush needed",
             "parallelism": "replicas (one LP per GPU)"}
 
@@ -447,7 +450,7 @@ def run(args, world, rank, local, dist):
             sa, sat = (int(v) for v in args.shapes.split(","))
             shapes = dict(spmv_shape_a=sa, spmv_shape_at=sat, autotune=0)
         r = V.solve(lp, precision=prec, iteration_limit=args.profile_iters, device=local,
-                    mixed_switch_tolerance=0.0, mixed_stall_checks=0, **shapes)
+                    mixed_switch_tolerance=0.0, mixed_stall_checks=0, degree_order=args.degree_order, **shapes)
         print(json.dumps({"profile_iters": r["iterations"], "status": r["status_name"], "rel_kkt": r["rel_kkt"],
                           "groups": [r["spmv_group_a"], r["spmv_group_at"]],
                           "primal_us": r["primal_kernel_us"], "dual_us": r["dual_kernel_us"],
@@ -468,7 +471,7 @@ def run(args, world, rank, local, dist):
         return float(t.item())
 
     # ---- mixed precision, resident LP ----------------------------------------------
-    solver = V.Solver(lp, precision=V.PREC_MIXED, device=local)
+    solver = V.Solver(lp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
     for _ in range(args.warmup):
         solver.run()
     barrier()
@@ -489,7 +492,7 @@ def run(args, world, rank, local, dist):
     # ---- plain FP64 form --------------------------------------------------------------
     fp64 = None
     if args.fp64_steps > 0:
-        s64 = V.Solver(lp, precision=V.PREC_FP64, device=local)
+        s64 = V.Solver(lp, precision=V.PREC_FP64, device=local, degree_order=args.degree_order)
         s64.run()
         r64 = [s64.run() for _ in range(args.fp64_steps)]
         s64.close()
@@ -504,7 +507,7 @@ def run(args, world, rank, local, dist):
         e2e_times = []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            r = V.solve(plp, precision=V.PREC_MIXED, device=local)
+            r = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
             e2e_times.append(time.perf_counter() - t0)
         barrier()
         h2d = 8 * (lp.num_cols + 1) + 12 * lp.nnz + 8 * (3 * lp.num_cols + 2 * lp.num_rows)

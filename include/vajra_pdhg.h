@@ -29,7 +29,7 @@ extern "C" {
 
 /* Layout version of the structs below.  A caller compiled against one version must not call
  * a library of another: compare with vajra_abi_version() before the first call. */
-#define VAJRA_ABI_VERSION 5
+#define VAJRA_ABI_VERSION 6
 
 typedef int32_t vajra_status;
 enum {
@@ -133,7 +133,12 @@ typedef struct vajra_opts {
                                    FP64 phase uses `reflection`.  Below 1 the reflected step is
                                    averaged, which keeps FP32 rounding noise from building up
                                    within a restart epoch                                 */
-    int32_t reserved[2];
+    int32_t degree_order;       /* HALPERN: renumber rows and columns by descending entry
+                                   count on the device, so that the vector entries the SpMVs
+                                   gather most often share cache lines; results come back in
+                                   the caller's numbering.  0 auto (on from 2^20 entries),
+                                   1 on, -1 off                                            */
+    int32_t reserved;
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and

@@ -212,3 +212,36 @@ def test_time_limit_stops_the_solve(cuda):
     g = V.solve(lp, precision=V.PREC_FP64, time_limit=1e-4)
     assert g["status_name"] == "TIME_LIMIT"
     assert g["iterations"] < 5000
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_degree_order_reaches_the_optimum(cuda, prec):
+    """Rows and columns renumbered by entry count on the device (forced on for a small LP with
+    2..40 entries a column): the solution comes back in the caller's numbering and passes every
+    check of the unordered solve."""
+    lp = W.random_planted(600, 1500, (2, 40), seed=31)
+    g = V.solve(lp, precision=prec, degree_order=1)
+    check_solution(lp, g, obj=lp.planted_objective)
+
+
+def test_degree_order_with_long_and_empty_rows_and_columns(cuda):
+    """The ordering with a row and a column longer than a row block and empty rows and columns.
+    FP64: on this LP the mixed solution (relative KKT 2.8e-7, ordered or not) leaves one
+    reduced cost 2 % above the reference verifier's absolute dual tolerance."""
+    base = W.small_random(2600, 3000, 12)
+    lp = with_structure(base, dense_row=7, dense_col=11, empty_rows=(3, 50, 2599), empty_cols=(0, 99, 2999), seed=1)
+    g = V.solve(lp, precision=V.PREC_FP64, degree_order=1)
+    check_solution(lp, g, obj=highs(lp))
+
+
+def test_degree_order_returns_the_callers_numbering(cuda):
+    """64 FP64 iterations with and without the ordering: the ordering changes summation orders
+    only, so the iterates agree to rounding; a wrong renumbering would differ at O(1)."""
+    lp = W.random_planted(1500, 4000, (2, 40), seed=33)
+    kw = dict(precision=V.PREC_FP64, iteration_limit=64, spmv_shape_a=-1, spmv_shape_at=-1)
+    a = V.solve(lp, degree_order=1, **kw)
+    b = V.solve(lp, degree_order=-1, **kw)
+    assert a["iterations"] == b["iterations"] == 64
+    for k in ("x", "y", "d", "row_value"):
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-7, atol=1e-9 * (1.0 + np.abs(b[k]).max()), err_msg=k)
+    assert abs(a["objective_value"] - b["objective_value"]) <= 1e-9 * (1.0 + abs(b["objective_value"]))

@@ -291,8 +291,11 @@ vajra_status vajra_pdhg_destroy(vajra_pdhg* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     {
-        vajra::DeviceLp empty;
+        vajra::DeviceLp empty, empty_ordered;
+        vajra::LpOrder empty_order;
         std::swap(h->lp, empty);   // frees device memory before the stream goes
+        std::swap(h->lp_ordered, empty_ordered);
+        std::swap(h->order, empty_order);
     }
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -494,8 +494,9 @@ void init_iterates(Phase<T>& ph, const Prepared& p, CheckBuffers& cb, cudaStream
 struct TuneKey {
     int device, m, n;
     int64_t nnz;
+    int ordered;
     bool operator<(const TuneKey& o) const {
-        return std::tie(device, m, n, nnz) < std::tie(o.device, o.m, o.n, o.nnz);
+        return std::tie(device, m, n, nnz, ordered) < std::tie(o.device, o.m, o.n, o.nnz, o.ordered);
     }
 };
 struct TuneEntry { int bits = 0, a32 = 8, at32 = 8, a64 = 8, at64 = 8; };
@@ -514,7 +515,15 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     const int64_t nnz = h->nnz;
     const bool is_max = h->sense != 0;
     const bool mixed = o.precision == VAJRA_PREC_MIXED;
-    const DeviceLp& lp = h->lp;
+    // Degree ordering (built once per handle); the result vectors go back to the caller's
+    // numbering at the end.  Below ~1M entries the vectors stay in cache anyway.
+    constexpr int64_t kOrderMinNnz = int64_t(1) << 20;
+    const bool ordered = o.degree_order > 0 || (o.degree_order == 0 && nnz >= kOrderMinNnz);
+    if (ordered && !h->ordered) {
+        VJ_TRY(order_by_degree(h->lp, h->lp_ordered, h->order, st));
+        h->ordered = true;
+    }
+    const DeviceLp& lp = ordered ? h->lp_ordered : h->lp;
 
     Prepared p;
     DeviceBuffer<SetupState> sst;
@@ -604,7 +613,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // Below ~1M entries a solve is launch-bound and the timing runs would cost more than any
     // shape saves: the set-up heuristic (lanes per row from the mean row length) stays.
     constexpr int64_t kAutotuneMinNnz = int64_t(1) << 20;
-    const TuneKey tkey{h->device, m, n, nnz};
+    const TuneKey tkey{h->device, m, n, nnz, ordered ? 1 : 0};
     if (o.autotune) {   // shapes another handle already tuned for this LP
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(tkey);
@@ -778,6 +787,25 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     k_dot_final<<<1, 1024, 0, st>>>(kCheckBlocks, cb.part_r.get(), h->objective_offset, obj.get());
     VJ_LAUNCH_CHECK();
     note_launch(cur_phase == 0 ? 6 : 4);
+    const double* out_x = x_out.get();
+    const double* out_row_value = row_value.get();
+    const double* out_y = y_out.get();
+    const double* out_col_dual = col_dual.get();
+    DeviceBuffer<double> ux, urv, uy, ucd;   // the caller's numbering
+    if (ordered) {
+        VJ_TRY(ux.alloc(n));
+        VJ_TRY(urv.alloc(m));
+        VJ_TRY(uy.alloc(m));
+        VJ_TRY(ucd.alloc(n));
+        VJ_TRY(unorder(n, h->order.col_order.get(), x_out.get(), ux.get(), st));
+        VJ_TRY(unorder(m, h->order.row_order.get(), row_value.get(), urv.get(), st));
+        VJ_TRY(unorder(m, h->order.row_order.get(), y_out.get(), uy.get(), st));
+        VJ_TRY(unorder(n, h->order.col_order.get(), col_dual.get(), ucd.get(), st));
+        out_x = ux.get();
+        out_row_value = urv.get();
+        out_y = uy.get();
+        out_col_dual = ucd.get();
+    }
     double objective = 0.0;
     VJ_CUDA(cudaMemcpyAsync(&objective, obj.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaMemcpyAsync(hs, S, sizeof(HState), cudaMemcpyDeviceToHost, st));
@@ -787,10 +815,10 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     dev_timer.stop(st);
     r->device_time_sec = dev_timer.seconds();
     const auto t_dl = Clock::now();
-    copy_out_vector(r->col_value, x_out.get(), n, st);
-    copy_out_vector(r->row_value, row_value.get(), m, st);
-    copy_out_vector(r->row_dual, y_out.get(), m, st);
-    copy_out_vector(r->col_dual, col_dual.get(), n, st);
+    copy_out_vector(r->col_value, out_x, n, st);
+    copy_out_vector(r->row_value, out_row_value, m, st);
+    copy_out_vector(r->row_dual, out_y, m, st);
+    copy_out_vector(r->col_dual, out_col_dual, n, st);
     VJ_CUDA(cudaStreamSynchronize(st));
     h->transfers += 4;
 

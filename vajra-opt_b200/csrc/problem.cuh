@@ -98,6 +98,19 @@ vajra_status spectral_norm_fast(const Prepared& p, int m, int n, int max_iter, d
 // may override `group`).
 vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st);
 
+// Degree ordering: columns and rows renumbered in descending order of their entry counts
+// (equal counts keep index order).  The entries of x and y that the two SpMVs gather most
+// often then sit together in a few cache lines instead of one line each, and the rows of a
+// row-block tile have similar lengths.  Within a column the entries keep their order.
+struct LpOrder {
+    DeviceBuffer<int32_t> col_order;   // new column -> caller's column
+    DeviceBuffer<int32_t> row_order;   // new row -> caller's row
+};
+vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, cudaStream_t st);
+
+// dst[order[k]] = src[k] for k < count: a result vector back in the caller's numbering.
+vajra_status unorder(int count, const int32_t* order, const double* src, double* dst, cudaStream_t st);
+
 // Row-block partition of `v` at `tile` entries per block: nb + 1 block boundaries, the nb
 // block descriptors, and the rows longer than `tile` (one CTA each).
 vajra_status build_row_partition(const CsrView& v, int64_t tile, DeviceBuffer<int32_t>& blocks,

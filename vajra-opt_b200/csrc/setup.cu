@@ -2,6 +2,7 @@
 // The reference runs all of this single-threaded on the host before the first iteration
 // (src/solvers/gpu/pdhg_cuda.cu:136-171); here it stays on the device.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <cmath>
 
@@ -562,6 +563,183 @@ vajra_status plan_spmv(const DeviceLp& lp, Prepared& p, cudaStream_t st) {
     (void)lp;
     VJ_TRY(plan_one(p.a, p.long_rows_a, p.rb_blocks_a, p.rb_tiles_a, p.rb_long_a, st));
     VJ_TRY(plan_one(p.at, p.long_rows_at, p.rb_blocks_at, p.rb_tiles_at, p.rb_long_at, st));
+    return VAJRA_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// degree ordering
+// ---------------------------------------------------------------------------------------
+// Sort keys: descending entry count as an ascending unsigned key (the stable radix sort keeps
+// equal counts in index order).
+__global__ void k_col_count_keys(int n, const int64_t* __restrict__ col_ptr, uint32_t* __restrict__ keys,
+                                 int32_t* __restrict__ idx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    keys[j] = 0xffffffffu - static_cast<uint32_t>(col_ptr[j + 1] - col_ptr[j]);
+    idx[j] = j;
+}
+
+__global__ void k_row_counts(int64_t nnz, const int32_t* __restrict__ row_idx, uint32_t* __restrict__ counts) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nnz;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        atomicAdd(&counts[row_idx[k]], 1u);
+}
+
+__global__ void k_row_count_keys(int m, uint32_t* __restrict__ keys, int32_t* __restrict__ idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    keys[i] = 0xffffffffu - keys[i];
+    idx[i] = i;
+}
+
+__global__ void k_invert(int count, const int32_t* __restrict__ order, int32_t* __restrict__ inv) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) inv[order[k]] = k;
+}
+
+// New column pointers: counts in the new order, then a running sum (one block).
+__global__ void k_ordered_counts(int n, const int64_t* __restrict__ col_ptr, const int32_t* __restrict__ col_order,
+                                 int64_t* __restrict__ counts) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) counts[k] = col_ptr[col_order[k] + 1] - col_ptr[col_order[k]];
+}
+
+// One warp per new column: its entries in the original order, rows renumbered.
+__global__ void k_copy_columns(int n, const int64_t* __restrict__ src_ptr, const int32_t* __restrict__ src_row,
+                               const double* __restrict__ src_val, const int32_t* __restrict__ col_order,
+                               const int32_t* __restrict__ row_inv, const int64_t* __restrict__ dst_ptr,
+                               int32_t* __restrict__ dst_row, double* __restrict__ dst_val) {
+    const int64_t w = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const int j = col_order[w];
+    const int64_t s = src_ptr[j], len = src_ptr[j + 1] - s, d = dst_ptr[w];
+    for (int64_t t = lane; t < len; t += 32) {
+        dst_row[d + t] = row_inv[src_row[s + t]];
+        dst_val[d + t] = src_val[s + t];
+    }
+}
+
+template <typename T>
+__global__ void k_take(int count, const int32_t* __restrict__ order, const T* __restrict__ src, T* __restrict__ dst) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) dst[k] = src[order[k]];
+}
+
+template <typename T>
+__global__ void k_put(int count, const int32_t* __restrict__ order, const T* __restrict__ src, T* __restrict__ dst) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) dst[order[k]] = src[k];
+}
+
+static vajra_status sort_order(int count, const uint32_t* keys, DeviceBuffer<int32_t>& idx,
+                               DeviceBuffer<int32_t>& order, cudaStream_t st) {
+    DeviceBuffer<uint32_t> keys_out;
+    VJ_TRY(keys_out.alloc(static_cast<size_t>(count)));
+    size_t temp_bytes = 0;
+    VJ_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, keys_out.get(), idx.get(), order.get(), count,
+                                            0, 32, st));
+    DeviceBuffer<unsigned char> temp;
+    VJ_TRY(temp.alloc(temp_bytes));
+    VJ_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), temp_bytes, keys, keys_out.get(), idx.get(), order.get(),
+                                            count, 0, 32, st));
+    note_launch(4);
+    VJ_CUDA(cudaStreamSynchronize(st));   // temporaries die here
+    return VAJRA_OK;
+}
+
+vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, cudaStream_t st) {
+    const int m = src.m, n = src.n;
+    const int64_t nnz = src.nnz;
+    dst.m = m;
+    dst.n = n;
+    dst.nnz = nnz;
+    dst.sense = src.sense;
+    dst.objective_offset = src.objective_offset;
+    VJ_TRY(ord.col_order.alloc(static_cast<size_t>(n)));
+    VJ_TRY(ord.row_order.alloc(static_cast<size_t>(m)));
+    DeviceBuffer<uint32_t> keys;
+    DeviceBuffer<int32_t> idx, row_inv;
+    // columns
+    VJ_TRY(keys.alloc(static_cast<size_t>(n)));
+    VJ_TRY(idx.alloc(static_cast<size_t>(n)));
+    if (n > 0) {
+        k_col_count_keys<<<grid_for(n), kThreads, 0, st>>>(n, src.col_ptr.get(), keys.get(), idx.get());
+        VJ_LAUNCH_CHECK();
+        note_launch(1);
+        VJ_TRY(sort_order(n, keys.get(), idx, ord.col_order, st));
+    }
+    // rows
+    VJ_TRY(keys.alloc(static_cast<size_t>(m)));
+    VJ_TRY(idx.alloc(static_cast<size_t>(m)));
+    VJ_TRY(row_inv.alloc(static_cast<size_t>(m)));
+    if (m > 0) {
+        VJ_CUDA(cudaMemsetAsync(keys.get(), 0, sizeof(uint32_t) * m, st));
+        if (nnz > 0) k_row_counts<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, src.row_idx.get(), keys.get());
+        k_row_count_keys<<<grid_for(m), kThreads, 0, st>>>(m, keys.get(), idx.get());
+        VJ_LAUNCH_CHECK();
+        note_launch(nnz > 0 ? 2 : 1);
+        VJ_TRY(sort_order(m, keys.get(), idx, ord.row_order, st));
+        k_invert<<<grid_for(m), kThreads, 0, st>>>(m, ord.row_order.get(), row_inv.get());
+        VJ_LAUNCH_CHECK();
+        note_launch(1);
+    }
+    // matrix: new column pointers, then the columns' entries with renumbered rows
+    VJ_TRY(dst.col_ptr.alloc(static_cast<size_t>(n) + 1));
+    VJ_TRY(dst.row_idx.alloc(static_cast<size_t>(nnz)));
+    VJ_TRY(dst.values.alloc(static_cast<size_t>(nnz)));
+    {
+        DeviceBuffer<int64_t> counts;
+        VJ_TRY(counts.alloc(static_cast<size_t>(n) + 1));
+        VJ_CUDA(cudaMemsetAsync(counts.get(), 0, sizeof(int64_t) * (static_cast<size_t>(n) + 1), st));
+        if (n > 0) {
+            k_ordered_counts<<<grid_for(n), kThreads, 0, st>>>(n, src.col_ptr.get(), ord.col_order.get(), counts.get());
+            VJ_LAUNCH_CHECK();
+            note_launch(1);
+        }
+        // exclusive sum over n + 1 slots (the last count is 0): col_ptr[0] = 0, col_ptr[n] = nnz
+        size_t temp_bytes = 0;
+        VJ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, counts.get(), dst.col_ptr.get(), n + 1, st));
+        DeviceBuffer<unsigned char> temp;
+        VJ_TRY(temp.alloc(temp_bytes));
+        VJ_CUDA(cub::DeviceScan::ExclusiveSum(temp.get(), temp_bytes, counts.get(), dst.col_ptr.get(), n + 1, st));
+        note_launch(2);
+        if (n > 0 && nnz > 0) {
+            k_copy_columns<<<grid_for(static_cast<int64_t>(n) * 32), kThreads, 0, st>>>(
+                n, src.col_ptr.get(), src.row_idx.get(), src.values.get(), ord.col_order.get(), row_inv.get(),
+                dst.col_ptr.get(), dst.row_idx.get(), dst.values.get());
+            VJ_LAUNCH_CHECK();
+            note_launch(1);
+        }
+        VJ_CUDA(cudaStreamSynchronize(st));   // temporaries die here
+    }
+    // vectors
+    VJ_TRY(dst.c.alloc(static_cast<size_t>(n)));
+    VJ_TRY(dst.col_lower.alloc(static_cast<size_t>(n)));
+    VJ_TRY(dst.col_upper.alloc(static_cast<size_t>(n)));
+    VJ_TRY(dst.row_lower.alloc(static_cast<size_t>(m)));
+    VJ_TRY(dst.row_upper.alloc(static_cast<size_t>(m)));
+    if (n > 0) {
+        k_take<double><<<grid_for(n), kThreads, 0, st>>>(n, ord.col_order.get(), src.c.get(), dst.c.get());
+        k_take<double><<<grid_for(n), kThreads, 0, st>>>(n, ord.col_order.get(), src.col_lower.get(), dst.col_lower.get());
+        k_take<double><<<grid_for(n), kThreads, 0, st>>>(n, ord.col_order.get(), src.col_upper.get(), dst.col_upper.get());
+        note_launch(3);
+    }
+    if (m > 0) {
+        k_take<double><<<grid_for(m), kThreads, 0, st>>>(m, ord.row_order.get(), src.row_lower.get(), dst.row_lower.get());
+        k_take<double><<<grid_for(m), kThreads, 0, st>>>(m, ord.row_order.get(), src.row_upper.get(), dst.row_upper.get());
+        note_launch(2);
+    }
+    VJ_LAUNCH_CHECK();
+    VJ_CUDA(cudaStreamSynchronize(st));
+    return VAJRA_OK;
+}
+
+vajra_status unorder(int count, const int32_t* order, const double* src, double* dst, cudaStream_t st) {
+    if (count <= 0) return VAJRA_OK;
+    k_put<double><<<grid_for(count), kThreads, 0, st>>>(count, order, src, dst);
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
     return VAJRA_OK;
 }
 

@@ -24,6 +24,11 @@ struct vajra_pdhg {
     int tuned = 0;                       // bit 0: FP32 shapes tuned, bit 1: FP64 shapes tuned
     int tuned_a32 = 8, tuned_at32 = 8;   // lane groups (0 = row-block kernel)
     int tuned_a64 = 8, tuned_at64 = 8;
+    // The LP renumbered by descending row / column entry counts, built by the first HALPERN
+    // run that asks for it and kept with the handle.
+    bool ordered = false;
+    vajra::DeviceLp lp_ordered;
+    vajra::LpOrder order;
 };
 
 namespace vajra {

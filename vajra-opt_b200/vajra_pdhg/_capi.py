@@ -16,7 +16,7 @@ _fp = C.POINTER(C.c_float)
 _i64p = C.POINTER(C.c_int64)
 _i32p = C.POINTER(C.c_int32)
 
-ABI_VERSION = 5   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
+ABI_VERSION = 6   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
 
 # vajra_status
 OK, ERR_INVALID_ARGUMENT, ERR_NO_DEVICE, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_WAIT_TIMEOUT, ERR_INTERNAL = range(7)
@@ -43,7 +43,7 @@ class VajraOpts(C.Structure):
                 ("restart_artificial", C.c_double), ("primal_weight_smoothing", C.c_double),
                 ("step_safety", C.c_double), ("restart_metric", C.c_int32),
                 ("spmv_shape_a", C.c_int32), ("spmv_shape_at", C.c_int32),
-                ("mixed_reflection", C.c_double), ("reserved", C.c_int32 * 2)]
+                ("mixed_reflection", C.c_double), ("degree_order", C.c_int32), ("reserved", C.c_int32)]
 
 
 class VajraResult(C.Structure):
