@@ -73,22 +73,24 @@ def test_mixed_senses_vs_highs(cuda, prec, seed):
     check_solution(lp, g, obj=highs(lp))
 
 
+@pytest.mark.parametrize("order", [0, 1])
 @pytest.mark.parametrize("prec", PRECISIONS)
-def test_maximise_free_columns_vs_highs(cuda, prec):
+def test_maximise_free_columns_vs_highs(cuda, prec, order):
     lp = W.small_random(150, 400, 9)
     lp.sense = 1
     lp.c = -lp.c
     lp.objective_offset = 3.5
     lp.col_lower = lp.col_lower.copy(); lp.col_upper = lp.col_upper.copy()
     lp.col_lower[::11] = -INF
-    g = V.solve(lp, precision=prec)
+    g = V.solve(lp, precision=prec, degree_order=order)
     check_solution(lp, g, obj=highs(lp))
 
 
+@pytest.mark.parametrize("order", [0, 1])
 @pytest.mark.parametrize("prec", PRECISIONS)
-def test_min_cost_flow_vs_highs(cuda, prec):
+def test_min_cost_flow_vs_highs(cuda, prec, order):
     lp = W.min_cost_flow(nodes=2000, arcs=15000, seed=5)
-    g = V.solve(lp, precision=prec)
+    g = V.solve(lp, precision=prec, degree_order=order)
     check_solution(lp, g, obj=highs(lp))
 
 
