@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--profile-precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--shapes", default=None,
                     help="profiling: fixed SpMV launch shapes 'A,AT' (-1 row block, -2 row block with two load "
-                         "groups, 1..32 lanes per row; write --shapes=-2,-2) instead of autotuning, whose timings a "
+                         "groups, -3 sliced ELL, 1..32 lanes per row; write --shapes=-2,-2) instead of autotuning, whose timings a "
                          "profiler would distort")
     ap.add_argument("--degree-order", type=int, default=0, choices=[-1, 0, 1],
                     help="row / column renumbering by entry count: 0 auto (on from 2^20 entries), 1 on, -1 off")
@@ -498,7 +498,8 @@ def run(args, world, rank, local, dist):
         s64.close()
         fp64 = {"value": max_over_ranks(statistics.mean(r["device_time_sec"] for r in r64)),
                 "iterations": r64[-1]["iterations"], "rel_kkt": r64[-1]["rel_kkt"],
-                "status": r64[-1]["status_name"], "objective": r64[-1]["objective_value"]}
+                "status": r64[-1]["status_name"], "objective": r64[-1]["objective_value"],
+                "spmv_groups": {"A": r64[-1]["spmv_group_a"], "A^T": r64[-1]["spmv_group_at"]}}
 
     # ---- end to end through vajra_pdhg_solve with pinned host buffers ---------------
     e2e = None

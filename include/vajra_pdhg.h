@@ -127,7 +127,8 @@ typedef struct vajra_opts {
     int32_t spmv_shape_a;       /* HALPERN launch shape of the A x SpMV: 0 autotune (>= 2^20
                                    entries) or the set-up heuristic, -1 row-block kernel,
                                    -2 row-block kernel with two load groups per thread,
-                                   1..32 lanes per row (1, 2, 4, 8, 16, 32)                */
+                                   -3 sliced ELL (degree-ordered LPs; else the row-block
+                                   kernel), 1..32 lanes per row (1, 2, 4, 8, 16, 32)        */
     int32_t spmv_shape_at;      /* the same for the A^T y SpMV                           */
     double mixed_reflection;    /* MIXED: reflection coefficient of the FP32 phase (0.8); the
                                    FP64 phase uses `reflection`.  Below 1 the reflected step is
@@ -178,8 +179,8 @@ typedef struct vajra_result {
     int64_t host_device_transfers;
     int32_t spmv_group_a;       /* SpMV shape chosen for A x: 1..32 lanes per row, 0 the
                                    shared-memory row-block kernel, 64 the same with two load
-                                   groups per thread, -1 the exact in-order kernel of
-                                   VAJRA_ALGO_REFERENCE                                      */
+                                   groups per thread, 128 sliced ELL, -1 the exact in-order
+                                   kernel of VAJRA_ALGO_REFERENCE                            */
     int32_t spmv_group_at;      /* same for A^T y                                           */
     /* Live kernel timing (HALPERN): CUDA-event durations of the fused iteration kernels,
      * sampled on the solve's stream once per check interval, for the precision that ran

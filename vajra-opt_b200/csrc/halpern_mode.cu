@@ -14,6 +14,7 @@
 // original problem, the primal-weighted KKT for restarts (sufficient 0.2 / necessary 0.8 +
 // no progress / artificial 0.36 of total), the primal-weight update at restarts, and -- in
 // mixed precision -- the hand-over from the FP32 phase to the FP64 polish.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -353,6 +354,8 @@ struct Phase {
     DeviceBuffer<T> c, cl, cu, rl, ru;          // iteration copies in T (FP64: separate copies too)
     const T* csr_val = nullptr;
     const T* csc_val = nullptr;
+    const T* sell_val_a = nullptr;    // the same values in sliced-ELL order (degree-ordered LPs)
+    const T* sell_val_at = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // around the first iteration of a chunk
@@ -382,17 +385,25 @@ struct Phase {
 };
 
 // `timed`: bracket the two kernels with event-record nodes (captured into the chunk graph).
+// One SpMV of an iteration in shape v.group; the sliced-ELL shape reads its own copy of the
+// values (`sell_val`), every other shape the CSR-order ones.
+template <typename T, class Epi>
+void launch_iter(const CsrView& v, const T* csr_val, const T* sell_val, const T* x, Epi epi, cudaStream_t st) {
+    if (v.group == kSell && v.sell_off && sell_val) launch_sell<T, T, T>(v, csr_val, sell_val, x, epi, st);
+    else launch_spmv_t<T, T, T>(v, csr_val, x, epi, st);
+}
+
 template <typename T>
 void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, const double* hw, double gamma, int kk,
                        int write_cand, bool timed, cudaStream_t st) {
     if (timed) cudaEventRecordWithFlags(ph.ev[0], st, cudaEventRecordExternal);
-    launch_spmv_t<T, T, T>(at, ph.csc_val, ph.y.get(),
-                           EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                         ph.xc.get(), ph.xprev.get(), S, hw, gamma, kk, ph.phase, write_cand}, st);
+    launch_iter<T>(at, ph.csc_val, ph.sell_val_at, ph.y.get(),
+                   EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
+                                 ph.xc.get(), ph.xprev.get(), S, hw, gamma, kk, ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[1], st, cudaEventRecordExternal);
-    launch_spmv_t<T, T, T>(a, ph.csr_val, ph.xb.get(),
-                           EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, gamma, kk,
-                                       ph.phase, write_cand}, st);
+    launch_iter<T>(a, ph.csr_val, ph.sell_val_a, ph.xb.get(),
+                   EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, gamma, kk,
+                               ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[2], st, cudaEventRecordExternal);
 }
 
@@ -447,34 +458,57 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
     VJ_CUDA(cudaEventCreate(&e0));
     VJ_CUDA(cudaEventCreate(&e1));
     struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
+    // Every shape: one warm launch and three timed ones.  The three fastest then run three
+    // more rounds of four launches each, taking turns (so a drift of the clock or of the
+    // neighbours' load spreads over all of them), and the smallest total wins: shapes a few
+    // per cent apart are not told apart by one three-launch sample.
     auto time_shapes = [&](CsrView& v, auto launch) -> vajra_status {
         if (v.rows <= 0) return VAJRA_OK;
-        float best = 1e30f;
-        int best_g = v.group;
-        for (int g : {0, kRowblock2, 1, 2, 4, 8, 16, 32}) {
+        constexpr int kFinal = 3;
+        int shapes[9] = {0, kRowblock2, 1, 2, 4, 8, 16, 32, kSell};
+        const int kShapes = v.sell_off ? 9 : 8;
+        auto timed = [&](int g, int launches, float* ms) -> vajra_status {
             CsrView t = v;
             t.group = g;
-            launch(t);   // warm
             VJ_CUDA(cudaEventRecord(e0, st));
-            for (int r = 0; r < 3; ++r) launch(t);
+            for (int r = 0; r < launches; ++r) launch(t);
             VJ_CUDA(cudaEventRecord(e1, st));
             VJ_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            VJ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) { best = ms; best_g = g; }
+            VJ_CUDA(cudaEventElapsedTime(ms, e0, e1));
+            return VAJRA_OK;
+        };
+        float first[9];
+        for (int i = 0; i < kShapes; ++i) {
+            CsrView t = v;
+            t.group = shapes[i];
+            launch(t);   // warm
+            VJ_TRY(timed(shapes[i], 3, &first[i]));
         }
-        v.group = best_g;
+        int order[9];
+        for (int i = 0; i < kShapes; ++i) order[i] = i;
+        std::sort(order, order + kShapes, [&](int a, int b) { return first[a] < first[b]; });
+        float total[kFinal] = {0.f, 0.f, 0.f};
+        for (int round = 0; round < 3; ++round)
+            for (int f = 0; f < kFinal; ++f) {
+                float ms = 0.f;
+                VJ_TRY(timed(shapes[order[f]], 4, &ms));
+                total[f] += ms;
+            }
+        int best = 0;
+        for (int f = 1; f < kFinal; ++f)
+            if (total[f] < total[best]) best = f;
+        v.group = shapes[order[best]];
         return VAJRA_OK;
     };
     VJ_TRY(time_shapes(at, [&](const CsrView& t) {
-        launch_spmv_t<T, T, T>(t, ph.csc_val, ph.y.get(),
-                               EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                             ph.xc.get(), ph.xprev.get(), tune_state, hw, gamma, 0, ph.phase, 0}, st);
+        launch_iter<T>(t, ph.csc_val, ph.sell_val_at, ph.y.get(),
+                       EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
+                                     ph.xc.get(), ph.xprev.get(), tune_state, hw, gamma, 0, ph.phase, 0}, st);
     }));
     VJ_TRY(time_shapes(a, [&](const CsrView& t) {
-        launch_spmv_t<T, T, T>(t, ph.csr_val, ph.xb.get(),
-                               EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
-                                           tune_state, hw, gamma, 0, ph.phase, 0}, st);
+        launch_iter<T>(t, ph.csr_val, ph.sell_val_a, ph.xb.get(),
+                       EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
+                                   tune_state, hw, gamma, 0, ph.phase, 0}, st);
     }));
     return VAJRA_OK;
 }
@@ -547,6 +581,12 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         return VAJRA_OK;
     }
     if (mixed) VJ_TRY(make_f32_values(p, nnz, st));
+    // Sliced-ELL copies of both matrices (their rows are sorted by length only after the
+    // degree ordering): one more launch shape for the autotuner.
+    if (ordered) {
+        VJ_TRY(build_sell(p.a, p.csr_val.get(), mixed ? p.csr_val32.get() : nullptr, p.sell_a, st));
+        VJ_TRY(build_sell(p.at, p.csc_val.get(), mixed ? p.csc_val32.get() : nullptr, p.sell_at, st));
+    }
 
     // Norms for the relative KKT and the initial primal weight.
     DeviceBuffer<double> norms;
@@ -570,10 +610,14 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         VJ_TRY(p32.alloc(m, n, p, st));
         p32.csr_val = p.csr_val32.get();
         p32.csc_val = p.csc_val32.get();
+        p32.sell_val_a = p.a.sell_off ? p.sell_a.val32.get() : nullptr;
+        p32.sell_val_at = p.at.sell_off ? p.sell_at.val32.get() : nullptr;
     }
     VJ_TRY(p64.alloc(m, n, p, st));
     p64.csr_val = p.csr_val.get();
     p64.csc_val = p.csc_val.get();
+    p64.sell_val_a = p.a.sell_off ? p.sell_a.val64.get() : nullptr;
+    p64.sell_val_at = p.at.sell_off ? p.sell_at.val64.get() : nullptr;
 
     CheckBuffers cb;
     VJ_TRY(cb.ax.alloc(m));
@@ -661,6 +705,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         if (shape == -1 || shape == -2 || shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16 ||
             shape == 32)
             v32.group = v64.group = shape == -1 ? 0 : (shape == -2 ? kRowblock2 : shape);
+        if (shape == -3) v32.group = v64.group = v32.sell_off ? kSell : 0;   // sliced ELL, else row block
     };
     forced(o.spmv_shape_a, a32, a64);
     forced(o.spmv_shape_at, at32, at64);

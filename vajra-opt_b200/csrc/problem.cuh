@@ -27,6 +27,15 @@ struct DeviceLp {
     DeviceBuffer<double> c, col_lower, col_upper, row_lower, row_upper;
 };
 
+// Sliced-ELL copy of a matrix whose rows are sorted by descending length (spmv.cuh, kSell):
+// slice offsets, indices, and the values in FP64 and (mixed precision) FP32.
+struct SellData {
+    DeviceBuffer<int64_t> off;
+    DeviceBuffer<int32_t> idx;
+    DeviceBuffer<double> val64;
+    DeviceBuffer<float> val32;
+};
+
 struct Prepared {
     // structure
     DeviceBuffer<int64_t> csr_ptr;
@@ -43,6 +52,8 @@ struct Prepared {
     // row-block partitions (block boundaries) and their rows longer than kTile
     DeviceBuffer<int32_t> rb_blocks_a, rb_blocks_at, rb_long_a, rb_long_at;
     DeviceBuffer<TileDesc> rb_tiles_a, rb_tiles_at;
+    // sliced-ELL copies (degree-ordered LPs only)
+    SellData sell_a, sell_at;
     bool scaled = false;
     CsrView a, at;                            // A (rows = m) and A^T (rows = n)
 };
@@ -107,6 +118,11 @@ struct LpOrder {
     DeviceBuffer<int32_t> row_order;   // new row -> caller's row
 };
 vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, cudaStream_t st);
+
+// Sliced-ELL copy (SellData) of a matrix whose rows are sorted by descending length.
+// Builds `out` for `v` from its CSR-order values (val32 may be null) and sets v's sell_*
+// fields; leaves `v` without them when its rows are not in descending order of length.
+vajra_status build_sell(CsrView& v, const double* val64, const float* val32, SellData& out, cudaStream_t st);
 
 // dst[order[k]] = src[k] for k < count: a result vector back in the caller's numbering.
 vajra_status unorder(int count, const int32_t* order, const double* src, double* dst, cudaStream_t st);

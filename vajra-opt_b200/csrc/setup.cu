@@ -735,6 +735,98 @@ vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, c
     return VAJRA_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// sliced ELL
+// ---------------------------------------------------------------------------------------
+// info[0]: 1 when some row is longer than the row before it; info[1] / info[2]: rows longer
+// than kSellWidth / kSellCtaRow (a prefix when the rows are sorted).
+__global__ void k_sell_scan_rows(int rows, const int64_t* __restrict__ ptr, int* __restrict__ info) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const int64_t len = ptr[r + 1] - ptr[r];
+    if (r > 0 && len > ptr[r] - ptr[r - 1]) atomicOr(&info[0], 1);
+    if (len > kSellWidth) atomicAdd(&info[1], 1);
+    if (len > kSellCtaRow) atomicAdd(&info[2], 1);
+}
+
+// Slice s holds 32 x (its first row's length) slots; sizes[slices] = 0 closes the scan.
+__global__ void k_sell_sizes(int n_long, int slices, const int64_t* __restrict__ ptr, int64_t* __restrict__ sizes) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > slices) return;
+    if (s == slices) { sizes[s] = 0; return; }
+    const int r = n_long + 32 * s;
+    sizes[s] = 32 * (ptr[r + 1] - ptr[r]);
+}
+
+// One thread per sliced row: its entries to slots off[s] + 32 k + lane.
+__global__ void k_sell_fill(int rows, int n_long, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                            const double* __restrict__ v64, const float* __restrict__ v32,
+                            const int64_t* __restrict__ off, int32_t* __restrict__ sidx, double* __restrict__ s64,
+                            float* __restrict__ s32) {
+    const int r = n_long + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const int t = r - n_long, s = t >> 5, lane = t & 31;
+    const int64_t b = ptr[r], len = ptr[r + 1] - b, o = off[s] + lane;
+    for (int64_t k = 0; k < len; ++k) {
+        sidx[o + 32 * k] = idx[b + k];
+        s64[o + 32 * k] = v64[b + k];
+        if (v32) s32[o + 32 * k] = v32[b + k];
+    }
+}
+
+vajra_status build_sell(CsrView& v, const double* val64, const float* val32, SellData& out, cudaStream_t st) {
+    v.sell_off = nullptr;
+    v.sell_idx = nullptr;
+    v.sell_slices = v.sell_n_long = v.sell_n_vlong = 0;
+    if (v.rows <= 0) return VAJRA_OK;
+    DeviceBuffer<int> info;
+    VJ_TRY(info.alloc(3));
+    VJ_CUDA(cudaMemsetAsync(info.get(), 0, 3 * sizeof(int), st));
+    k_sell_scan_rows<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, info.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
+    int hi[3];
+    VJ_CUDA(cudaMemcpyAsync(hi, info.get(), sizeof(hi), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    if (hi[0]) return VAJRA_OK;   // rows not sorted: no sliced copy
+    const int n_long = hi[1], n_vlong = hi[2];
+    const int slices = (v.rows - n_long + 31) / 32;
+    VJ_TRY(out.off.alloc(static_cast<size_t>(slices) + 1));
+    {
+        DeviceBuffer<int64_t> sizes;
+        VJ_TRY(sizes.alloc(static_cast<size_t>(slices) + 1));
+        k_sell_sizes<<<grid_for(static_cast<int64_t>(slices) + 1), kThreads, 0, st>>>(n_long, slices, v.ptr, sizes.get());
+        VJ_LAUNCH_CHECK();
+        size_t temp_bytes = 0;
+        VJ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, sizes.get(), out.off.get(), slices + 1, st));
+        DeviceBuffer<unsigned char> temp;
+        VJ_TRY(temp.alloc(temp_bytes));
+        VJ_CUDA(cub::DeviceScan::ExclusiveSum(temp.get(), temp_bytes, sizes.get(), out.off.get(), slices + 1, st));
+        note_launch(3);
+        VJ_CUDA(cudaStreamSynchronize(st));   // temporaries die here
+    }
+    int64_t total = 0;
+    VJ_CUDA(cudaMemcpyAsync(&total, out.off.get() + slices, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    VJ_TRY(out.idx.alloc(static_cast<size_t>(total)));
+    VJ_TRY(out.val64.alloc(static_cast<size_t>(total)));
+    if (val32) VJ_TRY(out.val32.alloc(static_cast<size_t>(total)));
+    const int sliced_rows = v.rows - n_long;
+    if (sliced_rows > 0) {
+        k_sell_fill<<<grid_for(sliced_rows), kThreads, 0, st>>>(v.rows, n_long, v.ptr, v.idx, val64, val32,
+                                                                out.off.get(), out.idx.get(), out.val64.get(),
+                                                                val32 ? out.val32.get() : nullptr);
+        VJ_LAUNCH_CHECK();
+        note_launch(1);
+    }
+    v.sell_off = out.off.get();
+    v.sell_idx = out.idx.get();
+    v.sell_slices = slices;
+    v.sell_n_long = n_long;
+    v.sell_n_vlong = n_vlong;
+    return VAJRA_OK;
+}
+
 vajra_status unorder(int count, const int32_t* order, const double* src, double* dst, cudaStream_t st) {
     if (count <= 0) return VAJRA_OK;
     k_put<double><<<grid_for(count), kThreads, 0, st>>>(count, order, src, dst);

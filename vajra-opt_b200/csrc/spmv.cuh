@@ -334,6 +334,76 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
     }
 }
 
+// ----- sliced-ELL family (rows sorted by descending length) -----------------------------
+// For a matrix whose rows are numbered in descending order of length (the degree-ordered LP),
+// the rows up to kSellWidth entries are cut into slices of 32 consecutive rows, and slice s
+// stores entry k of its row `lane` at sell_off[s] + 32 k + lane: one warp takes a slice, a
+// thread its row, and every load of indices and values is one coalesced 128-byte line per
+// warp.  Rows of a slice have nearly equal lengths, so the slice's width (its first row's
+// length) wastes little and no shared memory, barrier or cross-lane reduction is needed; a
+// row's sum is formed in storage order.  The longer rows (a prefix) stay in CSR: one warp per
+// row, and one CTA per row above kSellCtaRow entries.  Padding slots are never read.
+constexpr int kSellWidth = 64;
+constexpr int kSellCtaRow = 4096;
+
+template <typename VV, typename VX, typename Acc, class Epi>
+__device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                                              const VV* __restrict__ val, const VX* __restrict__ x, const Epi& epi) {
+    const int lane = threadIdx.x & 31;
+    PreOf<Epi> pre{};
+    if (lane == 0) pre = epi_pre(epi, row, 0);
+    const int64_t s = ptr[row], e = ptr[row + 1];
+    Acc acc = Acc(0);
+#pragma unroll 4
+    for (int64_t k = s + lane; k < e; k += 32)
+        acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+    acc = warp_reduce<OpSum>(acc);
+    if (lane == 0) epi_fin(epi, row, acc, pre, 0);
+}
+
+// CTAs [0, n_vlong): rows [0, n_vlong), one CTA each.  Then 8 warps a CTA: warps [0, n_long -
+// n_vlong) take rows n_vlong.. one each, the following warps the slices.
+template <typename VV, typename VX, typename Acc, class Epi, int MB>
+__global__ void __launch_bounds__(kThreads, MB)
+k_spmv_sell(int rows, int n_vlong, int n_long, int slices, const int64_t* __restrict__ ptr,
+            const int32_t* __restrict__ idx, const VV* __restrict__ val, const int64_t* __restrict__ sell_off,
+            const int32_t* __restrict__ sell_idx, const VV* __restrict__ sell_val, const VX* __restrict__ x, Epi epi) {
+    if (!epi.active()) return;
+    if (static_cast<int>(blockIdx.x) < n_vlong) {
+        __shared__ Acc red[32];
+        const int row = blockIdx.x;
+        const int64_t s = ptr[row], e = ptr[row + 1];
+        Acc acc = Acc(0);
+        for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+        Acc v[1] = {acc};
+        block_reduce<OpSum, Acc, 1>(v, red);
+        if (threadIdx.x == 0) epi(row, v[0]);
+        return;
+    }
+    const int w = (static_cast<int>(blockIdx.x) - n_vlong) * (kThreads / 32) + static_cast<int>(threadIdx.x >> 5);
+    const int n_med = n_long - n_vlong;
+    if (w < n_med) {
+        sell_warp_row<VV, VX, Acc>(n_vlong + w, ptr, idx, val, x, epi);
+        return;
+    }
+    const int sl = w - n_med;
+    if (sl >= slices) return;
+    const int lane = threadIdx.x & 31;
+    const int row = n_long + sl * 32 + lane;
+    if (row >= rows) return;
+    const PreOf<Epi> pre = epi_pre(epi, row, 0);
+    const int len = static_cast<int>(ptr[row + 1] - ptr[row]);
+    const int64_t base = sell_off[sl] + lane;
+    Acc acc = Acc(0);
+#pragma unroll 4
+    for (int k = 0; k < len; ++k) {
+        const int64_t q = base + 32 * static_cast<int64_t>(k);
+        acc = fma(static_cast<Acc>(ld_stream(sell_val + q)), static_cast<Acc>(ld_cached(x + ld_stream(sell_idx + q))), acc);
+    }
+    epi_fin(epi, row, acc, pre, 0);
+}
+
 // Host-side description of one SpMV operand (a CSR, possibly the stored transpose) and the
 // launch shape the autotuner chose for it.
 struct CsrView {
@@ -356,7 +426,31 @@ struct CsrView {
     const int32_t* blk_list = nullptr;
     const int* blk_count = nullptr;
     int blk_grid = 0;
+    // Sliced-ELL structure (rows sorted by descending length only; null otherwise): rows
+    // [0, sell_n_vlong) one CTA each, [sell_n_vlong, sell_n_long) one warp each, the rest in
+    // sell_slices slices of 32 rows.  The values in that order are per precision and are
+    // passed to launch_sell by the caller.
+    const int64_t* sell_off = nullptr;
+    const int32_t* sell_idx = nullptr;
+    int sell_slices = 0;
+    int sell_n_long = 0;
+    int sell_n_vlong = 0;
 };
+
+// Launch-shape code of the sliced-ELL kernel.
+constexpr int kSell = 128;
+
+template <typename VV, typename VX, typename Acc, class Epi>
+inline void launch_sell(const CsrView& a, const VV* csr_val, const VV* sell_val, const VX* x, Epi epi, cudaStream_t st) {
+    constexpr int MB = sizeof(VV) == 4 ? 6 : 4;
+    const int warps = (a.sell_n_long - a.sell_n_vlong) + a.sell_slices;
+    const int blocks = a.sell_n_vlong + (warps + kThreads / 32 - 1) / (kThreads / 32);
+    if (blocks <= 0) return;
+    k_spmv_sell<VV, VX, Acc, Epi, MB><<<blocks, kThreads, 0, st>>>(
+        a.rows, a.sell_n_vlong, a.sell_n_long, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_off, a.sell_idx, sell_val,
+        x, epi);
+    note_launch();
+}
 
 // Launch-shape code of the row-block kernel with two groups of four entries in flight per
 // thread (U = 2).  With 4-byte values it keeps six CTAs per SM by leaving the epilogue's loads
@@ -388,10 +482,13 @@ inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, 
 }
 
 // group 0 / kRowblock2 select the row-block kernel; other lane-group sizes than 1..16 dispatch to 32.
+// kSell needs the values in sliced-ELL order (launch_sell); given CSR values only, it runs as
+// the row-block kernel.
 template <typename VV, typename VX, typename Acc, class Epi>
 inline void launch_spmv_t(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     if (a.rows <= 0) return;
     switch (a.group) {
+        case kSell:
         case 0:
             if (a.tiles) { launch_rowblock<VV, VX, Acc, 1>(a, val, x, epi, st); break; }
             launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st);
