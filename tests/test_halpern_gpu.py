@@ -261,11 +261,11 @@ def test_sliced_ell_shape_reaches_the_optimum(cuda, prec):
 
 def test_sliced_ell_long_rows_and_empty_rows_and_columns(cuda):
     """Sliced ELL with a row of ~5000 entries (one CTA), a column of ~2600 (one warp), rows
-    above 64 entries kept in CSR, and empty rows and columns."""
+    above 128 entries kept in CSR, and empty rows and columns."""
     base = W.small_random(2600, 5000, 12)
     lp = with_structure(base, dense_row=7, dense_col=11, empty_rows=(3, 50, 2599), empty_cols=(0, 99, 4999), seed=1)
     A = lp.to_scipy_csc()
-    assert np.diff(A.tocsr().indptr).max() > 4096 and np.diff(lp.col_ptr).max() > 64
+    assert np.diff(A.tocsr().indptr).max() > 4096 and np.diff(lp.col_ptr).max() > 128
     g = V.solve(lp, precision=V.PREC_FP64, degree_order=1, spmv_shape_a=-3, spmv_shape_at=-3)
     assert g["spmv_group_a"] == 128 and g["spmv_group_at"] == 128
     check_solution(lp, g, obj=highs(lp))
@@ -274,7 +274,7 @@ def test_sliced_ell_long_rows_and_empty_rows_and_columns(cuda):
 def test_sliced_ell_matches_row_blocks(cuda):
     """64 FP64 iterations in sliced ELL and in row blocks: only the summation order differs,
     so the iterates agree to rounding; a misplaced entry would differ at O(1)."""
-    lp = W.random_planted(2000, 4000, (2, 50), seed=34)   # rows of 25..77 entries: slices and warps
+    lp = W.random_planted(900, 4000, (2, 50), seed=34)   # rows on both sides of 128 entries: slices and warps
     kw = dict(precision=V.PREC_FP64, iteration_limit=64, degree_order=1)
     a = V.solve(lp, spmv_shape_a=-3, spmv_shape_at=-3, **kw)
     b = V.solve(lp, spmv_shape_a=-1, spmv_shape_at=-1, **kw)

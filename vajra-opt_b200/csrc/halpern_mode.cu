@@ -416,8 +416,17 @@ struct CheckBuffers {
 template <typename T>
 void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const Prepared& p, const DeviceLp& lp,
                    CheckBuffers& cb, HState* S, const ControlParams& cp, cudaStream_t st) {
-    launch_spmv_t<double, T, double>(a64, p.csr_val.get(), ph.xc.get(), EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
-    launch_spmv_t<double, T, double>(at64, p.csc_val.get(), ph.yc.get(), EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
+    // FP64 values of the scaled A; in sliced-ELL order too when that is the FP64 shape
+    if (a64.group == kSell && a64.sell_off)
+        launch_sell<double, T, double>(a64, p.csr_val.get(), p.sell_a.val64.get(), ph.xc.get(),
+                                       EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
+    else
+        launch_spmv_t<double, T, double>(a64, p.csr_val.get(), ph.xc.get(), EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
+    if (at64.group == kSell && at64.sell_off)
+        launch_sell<double, T, double>(at64, p.csc_val.get(), p.sell_at.val64.get(), ph.yc.get(),
+                                       EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
+    else
+        launch_spmv_t<double, T, double>(at64, p.csc_val.get(), ph.yc.get(), EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
     k_kkt_rows<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.m, cb.ax.get(), ph.yc.get(), ph.yprev.get(), p.row_lower.get(), p.row_upper.get(),
                                                      lp.row_lower.get(), lp.row_upper.get(), p.row_scale.get(),
                                                      cb.y_last.get(), cb.part_r.get(), S, ph.phase);
@@ -553,16 +562,24 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // numbering at the end.  Below ~1M entries the vectors stay in cache anyway.
     constexpr int64_t kOrderMinNnz = int64_t(1) << 20;
     const bool ordered = o.degree_order > 0 || (o.degree_order == 0 && nnz >= kOrderMinNnz);
+    // verbose: host time of each set-up step (the stream drained at each mark)
+    auto mark = [&](const char* what) {
+        if (!o.verbose) return;
+        cudaStreamSynchronize(st);
+        std::fprintf(stderr, "[vajra] set-up %-14s %8.1f ms\n", what, 1e3 * seconds_since(t_start));
+    };
     if (ordered && !h->ordered) {
         VJ_TRY(order_by_degree(h->lp, h->lp_ordered, h->order, st));
         h->ordered = true;
     }
     const DeviceLp& lp = ordered ? h->lp_ordered : h->lp;
+    mark("ordering");
 
     Prepared p;
     DeviceBuffer<SetupState> sst;
     VJ_TRY(sst.alloc(1));
     VJ_TRY(build_csr(lp, p, st));
+    mark("csr");
     ScalingOpts so;
     so.enable = o.enable_scaling != 0;
     so.ruiz_iterations = o.ruiz_iterations > 0 ? o.ruiz_iterations : 10;
@@ -570,8 +587,20 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     so.pock_chambolle = o.pock_chambolle != 0;
     so.negate_c = is_max;
     VJ_TRY(prepare_scaled(lp, p, so, sst.get(), st));
+    mark("scaling");
     VJ_TRY(plan_spmv(lp, p, st));
+    mark("partitions");
+    if (mixed) VJ_TRY(make_f32_values(p, nnz, st));
+    // Sliced-ELL copies of both matrices (their rows are sorted by length only after the
+    // degree ordering): one more launch shape for the autotuner, and the power
+    // iteration's SpMVs.
+    if (ordered) {
+        VJ_TRY(build_sell(p.a, p.csr_val.get(), mixed ? p.csr_val32.get() : nullptr, p.sell_a, st));
+        VJ_TRY(build_sell(p.at, p.csc_val.get(), mixed ? p.csc_val32.get() : nullptr, p.sell_at, st));
+    }
+    mark("sliced ell");
     VJ_TRY(spectral_norm_fast(p, m, n, 100, 1e-5, sst.get(), st));
+    mark("norm estimate");
     SetupState hss{};
     VJ_CUDA(cudaMemcpy(&hss, sst.get(), sizeof(hss), cudaMemcpyDeviceToHost));
     const double spectral_norm = hss.spectral_norm;
@@ -579,13 +608,6 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         r->status = kStatusNumerical;
         std::snprintf(r->status_message, sizeof(r->status_message), "invalid spectral norm estimate %g", spectral_norm);
         return VAJRA_OK;
-    }
-    if (mixed) VJ_TRY(make_f32_values(p, nnz, st));
-    // Sliced-ELL copies of both matrices (their rows are sorted by length only after the
-    // degree ordering): one more launch shape for the autotuner.
-    if (ordered) {
-        VJ_TRY(build_sell(p.a, p.csr_val.get(), mixed ? p.csr_val32.get() : nullptr, p.sell_a, st));
-        VJ_TRY(build_sell(p.at, p.csc_val.get(), mixed ? p.csc_val32.get() : nullptr, p.sell_at, st));
     }
 
     // Norms for the relative KKT and the initial primal weight.
@@ -619,6 +641,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     p64.sell_val_a = p.a.sell_off ? p.sell_a.val64.get() : nullptr;
     p64.sell_val_at = p.at.sell_off ? p.sell_at.val64.get() : nullptr;
 
+    mark("iterate buffers");
     CheckBuffers cb;
     VJ_TRY(cb.ax.alloc(m));
     VJ_TRY(cb.aty.alloc(n));
@@ -667,6 +690,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             if ((e.bits & 2) && !(h->tuned & 2)) { h->tuned_a64 = e.a64; h->tuned_at64 = e.at64; h->tuned |= 2; }
         }
     }
+    mark("shape lookup");
     if (o.autotune && nnz >= kAutotuneMinNnz && (!(h->tuned & 2) || (mixed && !(h->tuned & 1)))) {
         HState tune = init;
         if (mixed && !(h->tuned & 1)) {
@@ -721,6 +745,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_LAUNCH_CHECK();
     note_launch(1);
     VJ_CUDA(cudaStreamSynchronize(st));
+    mark("launch shapes");
     const double setup_time = seconds_since(t_start);
 
     HState* S = dstate.get();

@@ -447,8 +447,17 @@ vajra_status spectral_norm_fast(const Prepared& p, int m, int n, int max_iter, d
     VJ_TRY(part.alloc(nparts));
     const int* done = &sst->power_done;
     for (int it = 0; it < max_iter; ++it) {
-        launch_spmv<double, double>(p.a, p.csr_val.get(), v.get(), EpiStoreUnlessDone{w.get(), done}, st);
-        launch_spmv<double, double>(p.at, p.csc_val.get(), w.get(), EpiStoreUnlessDone{u.get(), done}, st);
+        // sliced-ELL copies, where the set-up built them, are the faster form of both SpMVs
+        if (p.a.sell_off)
+            launch_sell<double, double, double>(p.a, p.csr_val.get(), p.sell_a.val64.get(), v.get(),
+                                                EpiStoreUnlessDone{w.get(), done}, st);
+        else
+            launch_spmv<double, double>(p.a, p.csr_val.get(), v.get(), EpiStoreUnlessDone{w.get(), done}, st);
+        if (p.at.sell_off)
+            launch_sell<double, double, double>(p.at, p.csc_val.get(), p.sell_at.val64.get(), w.get(),
+                                                EpiStoreUnlessDone{u.get(), done}, st);
+        else
+            launch_spmv<double, double>(p.at, p.csc_val.get(), w.get(), EpiStoreUnlessDone{u.get(), done}, st);
         k_sumsq_partial<<<nparts, kThreads, 0, st>>>(n, u.get(), part.get(), sst);
         k_power_step_fast<<<1, kThreads, 0, st>>>(nparts, part.get(), tol, sst);
         k_power_scale<<<grid_for(n), kThreads, 0, st>>>(n, u.get(), v.get(), sst);

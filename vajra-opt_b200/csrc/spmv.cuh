@@ -343,7 +343,7 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
 // length) wastes little and no shared memory, barrier or cross-lane reduction is needed; a
 // row's sum is formed in storage order.  The longer rows (a prefix) stay in CSR: one warp per
 // row, and one CTA per row above kSellCtaRow entries.  Padding slots are never read.
-constexpr int kSellWidth = 64;
+constexpr int kSellWidth = 128;
 constexpr int kSellCtaRow = 4096;
 
 template <typename VV, typename VX, typename Acc, class Epi>
