@@ -248,9 +248,11 @@ vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra
         set_error("unknown algorithm %d", o.algorithm);
         return VAJRA_ERR_INVALID_ARGUMENT;
     }
+    const auto t_probe = Clock::now();
     vajra_device_info info;
     s = vajra_probe_device(o.device, &info);
     if (s != VAJRA_OK) { set_error("no usable CUDA device %d (no CPU fallback)", o.device); return VAJRA_ERR_NO_DEVICE; }
+    if (o.verbose) std::fprintf(stderr, "[vajra] create: device probe %.1f ms\n", 1e3 * seconds_since(t_probe));
     auto t0 = Clock::now();
     vajra_pdhg* h = new (std::nothrow) vajra_pdhg();
     if (!h) return VAJRA_ERR_INTERNAL;
@@ -282,6 +284,7 @@ vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra
         if (s != VAJRA_OK) return fail(s);
     }
     h->upload_time_sec = seconds_since(t0);
+    if (o.verbose) std::fprintf(stderr, "[vajra] create: stream, upload, checks %.1f ms\n", 1e3 * h->upload_time_sec);
     *handle = h;
     return VAJRA_OK;
 }
@@ -375,9 +378,15 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
         fail_result(r, s);
         return s;
     }
+    const double t_create = seconds_since(t0);
     s = vajra_pdhg_run(h, r);
+    const double t_run = seconds_since(t0);
+    const bool verbose = h->opts.verbose != 0;
     vajra_pdhg_destroy(h);
     r->total_time_sec = seconds_since(t0);
+    if (verbose)
+        std::fprintf(stderr, "[vajra] solve: create %.1f ms, run %.1f ms, destroy %.1f ms\n", 1e3 * t_create,
+                     1e3 * (t_run - t_create), 1e3 * (r->total_time_sec - t_run));
     g_last_timing.total_time_sec = r->total_time_sec;
     return s;
 }

@@ -764,10 +764,12 @@ __global__ void k_sell_sizes(int n_long, int slices, const int64_t* __restrict__
     if (s > slices) return;
     if (s == slices) { sizes[s] = 0; return; }
     const int r = n_long + 32 * s;
-    sizes[s] = 32 * (ptr[r + 1] - ptr[r]);
+    const int64_t w = ptr[r + 1] - ptr[r];
+    sizes[s] = 32 * ((w + kSellPack - 1) / kSellPack * kSellPack);
 }
 
-// One thread per sliced row: its entries to slots off[s] + 32 k + lane.
+// One thread per sliced row: its entries to their slots (kSellPack entries of a row side by
+// side, then the next lane's).
 __global__ void k_sell_fill(int rows, int n_long, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                             const double* __restrict__ v64, const float* __restrict__ v32,
                             const int64_t* __restrict__ off, int32_t* __restrict__ sidx, double* __restrict__ s64,
@@ -775,11 +777,12 @@ __global__ void k_sell_fill(int rows, int n_long, const int64_t* __restrict__ pt
     const int r = n_long + blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
     const int t = r - n_long, s = t >> 5, lane = t & 31;
-    const int64_t b = ptr[r], len = ptr[r + 1] - b, o = off[s] + lane;
+    const int64_t b = ptr[r], len = ptr[r + 1] - b, o = off[s] + kSellPack * lane;
     for (int64_t k = 0; k < len; ++k) {
-        sidx[o + 32 * k] = idx[b + k];
-        s64[o + 32 * k] = v64[b + k];
-        if (v32) s32[o + 32 * k] = v32[b + k];
+        const int64_t q = o + 32 * kSellPack * (k / kSellPack) + k % kSellPack;
+        sidx[q] = idx[b + k];
+        s64[q] = v64[b + k];
+        if (v32) s32[q] = v32[b + k];
     }
 }
 

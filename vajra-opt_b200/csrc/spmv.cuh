@@ -345,6 +345,12 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
 // row, and one CTA per row above kSellCtaRow entries.  Padding slots are never read.
 constexpr int kSellWidth = 128;
 constexpr int kSellCtaRow = 4096;
+// Entries of a row stored next to each other in a slice (1 or 2): with 2, slice s holds entry
+// k of row `lane` at off[s] + 64 (k / 2) + 2 lane + k % 2 and its width is rounded up to even.
+constexpr int kSellPack = 2;
+template <typename T> struct Pack2;
+template <> struct Pack2<float> { using type = float2; };
+template <> struct Pack2<double> { using type = double2; };
 
 template <typename VV, typename VX, typename Acc, class Epi>
 __device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
@@ -394,12 +400,29 @@ k_spmv_sell(int rows, int n_vlong, int n_long, int slices, const int64_t* __rest
     if (row >= rows) return;
     const PreOf<Epi> pre = epi_pre(epi, row, 0);
     const int len = static_cast<int>(ptr[row + 1] - ptr[row]);
-    const int64_t base = sell_off[sl] + lane;
     Acc acc = Acc(0);
+    if constexpr (kSellPack == 1) {
+        const int64_t base = sell_off[sl] + lane;
 #pragma unroll 4
-    for (int k = 0; k < len; ++k) {
-        const int64_t q = base + 32 * static_cast<int64_t>(k);
-        acc = fma(static_cast<Acc>(ld_stream(sell_val + q)), static_cast<Acc>(ld_cached(x + ld_stream(sell_idx + q))), acc);
+        for (int k = 0; k < len; ++k) {
+            const int64_t q = base + 32 * static_cast<int64_t>(k);
+            acc = fma(static_cast<Acc>(ld_stream(sell_val + q)), static_cast<Acc>(ld_cached(x + ld_stream(sell_idx + q))),
+                      acc);
+        }
+    } else {
+        // entries 2j and 2j + 1 of a row are adjacent: one 8-byte index load and one 8- or
+        // 16-byte value load per pair (the slot after an odd row's last entry is not gathered)
+        using VV2 = typename Pack2<VV>::type;
+        const int64_t base = sell_off[sl] + 2 * lane;
+        const int pairs = (len + 1) >> 1;
+#pragma unroll 4
+        for (int j = 0; j < pairs; ++j) {
+            const int64_t q = base + 64 * static_cast<int64_t>(j);
+            const int2 ii = __ldcs(reinterpret_cast<const int2*>(sell_idx + q));
+            const VV2 vv = __ldcs(reinterpret_cast<const VV2*>(sell_val + q));
+            acc = fma(static_cast<Acc>(vv.x), static_cast<Acc>(ld_cached(x + ii.x)), acc);
+            if (2 * j + 1 < len) acc = fma(static_cast<Acc>(vv.y), static_cast<Acc>(ld_cached(x + ii.y)), acc);
+        }
     }
     epi_fin(epi, row, acc, pre, 0);
 }
