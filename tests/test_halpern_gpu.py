@@ -283,10 +283,11 @@ def test_sliced_ell_matches_row_blocks(cuda):
         np.testing.assert_allclose(a[k], b[k], rtol=1e-7, atol=1e-9 * (1.0 + np.abs(b[k]).max()), err_msg=k)
 
 
-def test_sliced_ell_shape_without_ordering_runs_row_blocks(cuda):
-    """Without the degree ordering no sliced copy exists: a forced shape -3 runs (and reports)
-    the row-block kernel, and the solve is unchanged."""
-    lp = W.random_planted(600, 1500, (2, 40), seed=31)
+def test_sliced_ell_shape_without_ordering(cuda):
+    """Without the degree ordering a forced shape -3 builds the sliced copy over rows in their
+    own order (slices of uneven rows, long rows listed wherever they are) and solves the same."""
+    base = W.small_random(2600, 5000, 12)
+    lp = with_structure(base, dense_row=7, dense_col=11, empty_rows=(3, 50, 2599), empty_cols=(0, 99, 4999), seed=1)
     g = V.solve(lp, precision=V.PREC_FP64, degree_order=-1, spmv_shape_a=-3, spmv_shape_at=-3)
-    assert g["spmv_group_a"] == 0 and g["spmv_group_at"] == 0
-    check_solution(lp, g, obj=lp.planted_objective)
+    assert g["spmv_group_a"] == 128 and g["spmv_group_at"] == 128
+    check_solution(lp, g, obj=highs(lp))

@@ -591,10 +591,11 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(plan_spmv(lp, p, st));
     mark("partitions");
     if (mixed) VJ_TRY(make_f32_values(p, nnz, st));
-    // Sliced-ELL copies of both matrices (their rows are sorted by length only after the
-    // degree ordering): one more launch shape for the autotuner, and the power
-    // iteration's SpMVs.
-    if (ordered) {
+    // Sliced-ELL copies of both matrices (full slices need rows of similar length, which the
+    // degree ordering provides): one more launch shape for the autotuner, and the power
+    // iteration's SpMVs.  Without the ordering they are built only when a caller forces the
+    // shape.
+    if (ordered || o.spmv_shape_a == -3 || o.spmv_shape_at == -3) {
         VJ_TRY(build_sell(p.a, p.csr_val.get(), mixed ? p.csr_val32.get() : nullptr, p.sell_a, st));
         VJ_TRY(build_sell(p.at, p.csc_val.get(), mixed ? p.csc_val32.get() : nullptr, p.sell_at, st));
     }

@@ -34,6 +34,7 @@ struct SellData {
     DeviceBuffer<int32_t> idx;
     DeviceBuffer<double> val64;
     DeviceBuffer<float> val32;
+    DeviceBuffer<int32_t> long_rows, vlong_rows;   // rows kept in CSR (row order)
 };
 
 struct Prepared {
@@ -119,9 +120,8 @@ struct LpOrder {
 };
 vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, cudaStream_t st);
 
-// Sliced-ELL copy (SellData) of a matrix whose rows are sorted by descending length.
-// Builds `out` for `v` from its CSR-order values (val32 may be null) and sets v's sell_*
-// fields; leaves `v` without them when its rows are not in descending order of length.
+// Sliced-ELL copy (SellData) of `v`: builds `out` from v's CSR-order values (val32 may be
+// null) and sets v's sell_* fields.
 vajra_status build_sell(CsrView& v, const double* val64, const float* val32, SellData& out, cudaStream_t st);
 
 // dst[order[k]] = src[k] for k < count: a result vector back in the caller's numbering.

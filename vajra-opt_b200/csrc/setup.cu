@@ -3,6 +3,8 @@
 // (src/solvers/gpu/pdhg_cuda.cu:136-171); here it stays on the device.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <cmath>
 
@@ -747,37 +749,43 @@ vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, c
 // ---------------------------------------------------------------------------------------
 // sliced ELL
 // ---------------------------------------------------------------------------------------
-// info[0]: 1 when some row is longer than the row before it; info[1] / info[2]: rows longer
-// than kSellWidth / kSellCtaRow (a prefix when the rows are sorted).
-__global__ void k_sell_scan_rows(int rows, const int64_t* __restrict__ ptr, int* __restrict__ info) {
+// flags[r] = 1 for rows of kSellWidth..kSellCtaRow entries, 2 above; 0 for sliced rows.
+__global__ void k_sell_classify(int rows, const int64_t* __restrict__ ptr, uint8_t* __restrict__ is_long,
+                                uint8_t* __restrict__ is_vlong) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
     const int64_t len = ptr[r + 1] - ptr[r];
-    if (r > 0 && len > ptr[r] - ptr[r - 1]) atomicOr(&info[0], 1);
-    if (len > kSellWidth) atomicAdd(&info[1], 1);
-    if (len > kSellCtaRow) atomicAdd(&info[2], 1);
+    is_long[r] = (len > kSellWidth && len <= kSellCtaRow) ? 1 : 0;
+    is_vlong[r] = len > kSellCtaRow ? 1 : 0;
 }
 
-// Slice s holds 32 x (its first row's length) slots; sizes[slices] = 0 closes the scan.
-__global__ void k_sell_sizes(int n_long, int slices, const int64_t* __restrict__ ptr, int64_t* __restrict__ sizes) {
+// Slice s holds 32 x (its longest sliced row's length, rounded up to kSellPack) slots;
+// sizes[slices] = 0 closes the scan.
+__global__ void k_sell_sizes(int rows, int slices, const int64_t* __restrict__ ptr, int64_t* __restrict__ sizes) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s > slices) return;
     if (s == slices) { sizes[s] = 0; return; }
-    const int r = n_long + 32 * s;
-    const int64_t w = ptr[r + 1] - ptr[r];
+    int64_t w = 0;
+    const int r1 = 32 * s + 32 < rows ? 32 * s + 32 : rows;
+    for (int r = 32 * s; r < r1; ++r) {
+        const int64_t len = ptr[r + 1] - ptr[r];
+        if (len <= kSellWidth && len > w) w = len;
+    }
     sizes[s] = 32 * ((w + kSellPack - 1) / kSellPack * kSellPack);
 }
 
 // One thread per sliced row: its entries to their slots (kSellPack entries of a row side by
 // side, then the next lane's).
-__global__ void k_sell_fill(int rows, int n_long, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+__global__ void k_sell_fill(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
                             const double* __restrict__ v64, const float* __restrict__ v32,
                             const int64_t* __restrict__ off, int32_t* __restrict__ sidx, double* __restrict__ s64,
                             float* __restrict__ s32) {
-    const int r = n_long + blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
-    const int t = r - n_long, s = t >> 5, lane = t & 31;
-    const int64_t b = ptr[r], len = ptr[r + 1] - b, o = off[s] + kSellPack * lane;
+    const int64_t b = ptr[r], len = ptr[r + 1] - b;
+    if (len > kSellWidth) return;
+    const int s = r >> 5, lane = r & 31;
+    const int64_t o = off[s] + kSellPack * lane;
     for (int64_t k = 0; k < len; ++k) {
         const int64_t q = o + 32 * kSellPack * (k / kSellPack) + k % kSellPack;
         sidx[q] = idx[b + k];
@@ -786,28 +794,46 @@ __global__ void k_sell_fill(int rows, int n_long, const int64_t* __restrict__ pt
     }
 }
 
+// The rows whose flag is set, in row order.
+static vajra_status select_rows(int rows, const uint8_t* flags, DeviceBuffer<int32_t>& out, int* count, cudaStream_t st) {
+    DeviceBuffer<int> n_sel;
+    VJ_TRY(n_sel.alloc(1));
+    VJ_TRY(out.alloc(static_cast<size_t>(rows)));
+    thrust::counting_iterator<int32_t> first(0);
+    size_t temp_bytes = 0;
+    VJ_CUDA(cub::DeviceSelect::Flagged(nullptr, temp_bytes, first, flags, out.get(), n_sel.get(), rows, st));
+    DeviceBuffer<unsigned char> temp;
+    VJ_TRY(temp.alloc(temp_bytes));
+    VJ_CUDA(cub::DeviceSelect::Flagged(temp.get(), temp_bytes, first, flags, out.get(), n_sel.get(), rows, st));
+    note_launch(1);
+    VJ_CUDA(cudaMemcpyAsync(count, n_sel.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));   // temporaries die here
+    return VAJRA_OK;
+}
+
 vajra_status build_sell(CsrView& v, const double* val64, const float* val32, SellData& out, cudaStream_t st) {
     v.sell_off = nullptr;
     v.sell_idx = nullptr;
+    v.sell_long_rows = v.sell_vlong_rows = nullptr;
     v.sell_slices = v.sell_n_long = v.sell_n_vlong = 0;
     if (v.rows <= 0) return VAJRA_OK;
-    DeviceBuffer<int> info;
-    VJ_TRY(info.alloc(3));
-    VJ_CUDA(cudaMemsetAsync(info.get(), 0, 3 * sizeof(int), st));
-    k_sell_scan_rows<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, info.get());
-    VJ_LAUNCH_CHECK();
-    note_launch(1);
-    int hi[3];
-    VJ_CUDA(cudaMemcpyAsync(hi, info.get(), sizeof(hi), cudaMemcpyDeviceToHost, st));
-    VJ_CUDA(cudaStreamSynchronize(st));
-    if (hi[0]) return VAJRA_OK;   // rows not sorted: no sliced copy
-    const int n_long = hi[1], n_vlong = hi[2];
-    const int slices = (v.rows - n_long + 31) / 32;
+    int n_long = 0, n_vlong = 0;
+    {
+        DeviceBuffer<uint8_t> is_long, is_vlong;
+        VJ_TRY(is_long.alloc(static_cast<size_t>(v.rows)));
+        VJ_TRY(is_vlong.alloc(static_cast<size_t>(v.rows)));
+        k_sell_classify<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, is_long.get(), is_vlong.get());
+        VJ_LAUNCH_CHECK();
+        note_launch(1);
+        VJ_TRY(select_rows(v.rows, is_long.get(), out.long_rows, &n_long, st));
+        VJ_TRY(select_rows(v.rows, is_vlong.get(), out.vlong_rows, &n_vlong, st));
+    }
+    const int slices = (v.rows + 31) / 32;
     VJ_TRY(out.off.alloc(static_cast<size_t>(slices) + 1));
     {
         DeviceBuffer<int64_t> sizes;
         VJ_TRY(sizes.alloc(static_cast<size_t>(slices) + 1));
-        k_sell_sizes<<<grid_for(static_cast<int64_t>(slices) + 1), kThreads, 0, st>>>(n_long, slices, v.ptr, sizes.get());
+        k_sell_sizes<<<grid_for(static_cast<int64_t>(slices) + 1), kThreads, 0, st>>>(v.rows, slices, v.ptr, sizes.get());
         VJ_LAUNCH_CHECK();
         size_t temp_bytes = 0;
         VJ_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, sizes.get(), out.off.get(), slices + 1, st));
@@ -823,18 +849,16 @@ vajra_status build_sell(CsrView& v, const double* val64, const float* val32, Sel
     VJ_TRY(out.idx.alloc(static_cast<size_t>(total)));
     VJ_TRY(out.val64.alloc(static_cast<size_t>(total)));
     if (val32) VJ_TRY(out.val32.alloc(static_cast<size_t>(total)));
-    const int sliced_rows = v.rows - n_long;
-    if (sliced_rows > 0) {
-        k_sell_fill<<<grid_for(sliced_rows), kThreads, 0, st>>>(v.rows, n_long, v.ptr, v.idx, val64, val32,
-                                                                out.off.get(), out.idx.get(), out.val64.get(),
-                                                                val32 ? out.val32.get() : nullptr);
-        VJ_LAUNCH_CHECK();
-        note_launch(1);
-    }
+    k_sell_fill<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, v.idx, val64, val32, out.off.get(), out.idx.get(),
+                                                       out.val64.get(), val32 ? out.val32.get() : nullptr);
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
     v.sell_off = out.off.get();
     v.sell_idx = out.idx.get();
     v.sell_slices = slices;
+    v.sell_long_rows = out.long_rows.get();
     v.sell_n_long = n_long;
+    v.sell_vlong_rows = out.vlong_rows.get();
     v.sell_n_vlong = n_vlong;
     return VAJRA_OK;
 }

@@ -334,19 +334,19 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
     }
 }
 
-// ----- sliced-ELL family (rows sorted by descending length) -----------------------------
-// For a matrix whose rows are numbered in descending order of length (the degree-ordered LP),
-// the rows up to kSellWidth entries are cut into slices of 32 consecutive rows, and slice s
-// stores entry k of its row `lane` at sell_off[s] + 32 k + lane: one warp takes a slice, a
-// thread its row, and every load of indices and values is one coalesced 128-byte line per
-// warp.  Rows of a slice have nearly equal lengths, so the slice's width (its first row's
-// length) wastes little and no shared memory, barrier or cross-lane reduction is needed; a
-// row's sum is formed in storage order.  The longer rows (a prefix) stay in CSR: one warp per
-// row, and one CTA per row above kSellCtaRow entries.  Padding slots are never read.
+// ----- sliced-ELL family ---------------------------------------------------------------
+// The rows are cut into slices of 32 consecutive rows; slice s stores entries 2j and 2j + 1 of
+// its row `lane` side by side at sell_off[s] + 64 j + 2 lane (kSellPack = 2; with 1, entry k at
+// sell_off[s] + 32 k + lane).  One warp takes a slice, a thread its row, and every load of
+// indices and values is coalesced across the warp; a row's sum is formed in storage order, so
+// no shared memory, barrier or cross-lane reduction is needed.  A slice's width is the length
+// of its longest row (rounded up to even); the padding is never gathered.  Rows longer than
+// kSellWidth stay in CSR and are listed: one warp each, one CTA each above kSellCtaRow
+// entries.  The layout pays off when the rows of a slice have similar lengths -- the
+// degree-ordered LP numbers its rows by descending length, so there the long rows are a prefix
+// and the slices are nearly full.
 constexpr int kSellWidth = 128;
 constexpr int kSellCtaRow = 4096;
-// Entries of a row stored next to each other in a slice (1 or 2): with 2, slice s holds entry
-// k of row `lane` at off[s] + 64 (k / 2) + 2 lane + k % 2 and its width is rounded up to even.
 constexpr int kSellPack = 2;
 template <typename T> struct Pack2;
 template <> struct Pack2<float> { using type = float2; };
@@ -367,39 +367,18 @@ __device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict
     if (lane == 0) epi_fin(epi, row, acc, pre, 0);
 }
 
-// CTAs [0, n_vlong): rows [0, n_vlong), one CTA each.  Then 8 warps a CTA: warps [0, n_long -
-// n_vlong) take rows n_vlong.. one each, the following warps the slices.
-template <typename VV, typename VX, typename Acc, class Epi, int MB>
-__global__ void __launch_bounds__(kThreads, MB)
-k_spmv_sell(int rows, int n_vlong, int n_long, int slices, const int64_t* __restrict__ ptr,
-            const int32_t* __restrict__ idx, const VV* __restrict__ val, const int64_t* __restrict__ sell_off,
-            const int32_t* __restrict__ sell_idx, const VV* __restrict__ sell_val, const VX* __restrict__ x, Epi epi) {
-    if (!epi.active()) return;
-    if (static_cast<int>(blockIdx.x) < n_vlong) {
-        __shared__ Acc red[32];
-        const int row = blockIdx.x;
-        const int64_t s = ptr[row], e = ptr[row + 1];
-        Acc acc = Acc(0);
-        for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
-            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
-        Acc v[1] = {acc};
-        block_reduce<OpSum, Acc, 1>(v, red);
-        if (threadIdx.x == 0) epi(row, v[0]);
-        return;
-    }
-    const int w = (static_cast<int>(blockIdx.x) - n_vlong) * (kThreads / 32) + static_cast<int>(threadIdx.x >> 5);
-    const int n_med = n_long - n_vlong;
-    if (w < n_med) {
-        sell_warp_row<VV, VX, Acc>(n_vlong + w, ptr, idx, val, x, epi);
-        return;
-    }
-    const int sl = w - n_med;
-    if (sl >= slices) return;
+// The rows of slice `sl` (one per lane) that are not listed as long.  No warp collectives.
+template <typename VV, typename VX, typename Acc, class Epi>
+__device__ __forceinline__ void sell_slice(int sl, int rows, const int64_t* __restrict__ ptr,
+                                           const int64_t* __restrict__ sell_off, const int32_t* __restrict__ sell_idx,
+                                           const VV* __restrict__ sell_val, const VX* __restrict__ x, const Epi& epi) {
     const int lane = threadIdx.x & 31;
-    const int row = n_long + sl * 32 + lane;
+    const int row = sl * 32 + lane;
     if (row >= rows) return;
+    const int64_t len64 = ptr[row + 1] - ptr[row];
+    if (len64 > kSellWidth) return;
+    const int len = static_cast<int>(len64);
     const PreOf<Epi> pre = epi_pre(epi, row, 0);
-    const int len = static_cast<int>(ptr[row + 1] - ptr[row]);
     Acc acc = Acc(0);
     if constexpr (kSellPack == 1) {
         const int64_t base = sell_off[sl] + lane;
@@ -410,8 +389,8 @@ k_spmv_sell(int rows, int n_vlong, int n_long, int slices, const int64_t* __rest
                       acc);
         }
     } else {
-        // entries 2j and 2j + 1 of a row are adjacent: one 8-byte index load and one 8- or
-        // 16-byte value load per pair (the slot after an odd row's last entry is not gathered)
+        // one 8-byte index load and one 8- or 16-byte value load per pair (the slot after an
+        // odd row's last entry is not gathered)
         using VV2 = typename Pack2<VV>::type;
         const int64_t base = sell_off[sl] + 2 * lane;
         const int pairs = (len + 1) >> 1;
@@ -425,6 +404,47 @@ k_spmv_sell(int rows, int n_vlong, int n_long, int slices, const int64_t* __rest
         }
     }
     epi_fin(epi, row, acc, pre, 0);
+}
+
+// CTAs [0, n_vlong): the listed rows above kSellCtaRow entries, one CTA each.  The next
+// ceil(n_long / 8) CTAs: the listed rows of kSellWidth..kSellCtaRow entries, one warp each.
+// The remaining CTAs: 8 slices each, a warp per slice.  Long rows come first so that they
+// start first.
+template <typename VV, typename VX, typename Acc, class Epi, int MB>
+__global__ void __launch_bounds__(kThreads, MB)
+k_spmv_sell(int rows, int slices, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+            const VV* __restrict__ val, const int32_t* __restrict__ vlong_rows, int n_vlong,
+            const int32_t* __restrict__ long_rows, int n_long, const int64_t* __restrict__ sell_off,
+            const int32_t* __restrict__ sell_idx, const VV* __restrict__ sell_val, const VX* __restrict__ x, Epi epi) {
+    if (!epi.active()) return;
+    int b = static_cast<int>(blockIdx.x);
+    if (b < n_vlong) {
+        __shared__ Acc red[32];
+        const int row = vlong_rows[b];
+        if (skip_rows_impl(epi, row, row + 1, 0)) return;
+        const int64_t s = ptr[row], e = ptr[row + 1];
+        Acc acc = Acc(0);
+        for (int64_t k = s + threadIdx.x; k < e; k += blockDim.x)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+        Acc v[1] = {acc};
+        block_reduce<OpSum, Acc, 1>(v, red);
+        if (threadIdx.x == 0) epi(row, v[0]);
+        return;
+    }
+    b -= n_vlong;
+    const int warp = static_cast<int>(threadIdx.x >> 5);
+    constexpr int kWarps = kThreads / 32;
+    const int long_ctas = (n_long + kWarps - 1) / kWarps;
+    if (b < long_ctas) {
+        const int w = b * kWarps + warp;
+        if (w < n_long) {
+            const int row = long_rows[w];
+            if (!skip_rows_impl(epi, row, row + 1, 0)) sell_warp_row<VV, VX, Acc>(row, ptr, idx, val, x, epi);
+        }
+        return;
+    }
+    const int sl = (b - long_ctas) * kWarps + warp;
+    if (sl < slices) sell_slice<VV, VX, Acc>(sl, rows, ptr, sell_off, sell_idx, sell_val, x, epi);
 }
 
 // Host-side description of one SpMV operand (a CSR, possibly the stored transpose) and the
@@ -449,29 +469,34 @@ struct CsrView {
     const int32_t* blk_list = nullptr;
     const int* blk_count = nullptr;
     int blk_grid = 0;
-    // Sliced-ELL structure (rows sorted by descending length only; null otherwise): rows
-    // [0, sell_n_vlong) one CTA each, [sell_n_vlong, sell_n_long) one warp each, the rest in
-    // sell_slices slices of 32 rows.  The values in that order are per precision and are
-    // passed to launch_sell by the caller.
+    // Sliced-ELL structure (null where none was built): sell_slices slices of 32 rows, and the
+    // rows longer than kSellWidth listed (sell_long_rows: one warp each, sell_vlong_rows: above
+    // kSellCtaRow entries, one CTA each).  The values in slice order are per precision and
+    // are passed to launch_sell by the caller.
     const int64_t* sell_off = nullptr;
     const int32_t* sell_idx = nullptr;
     int sell_slices = 0;
+    const int32_t* sell_long_rows = nullptr;
     int sell_n_long = 0;
+    const int32_t* sell_vlong_rows = nullptr;
     int sell_n_vlong = 0;
 };
 
 // Launch-shape code of the sliced-ELL kernel.
 constexpr int kSell = 128;
 
+// Slice blocks (8 slices, one CTA) of the sliced-ELL kernel.
+inline int sell_block_count(const CsrView& a) { return (a.sell_slices + kThreads / 32 - 1) / (kThreads / 32); }
+
 template <typename VV, typename VX, typename Acc, class Epi>
 inline void launch_sell(const CsrView& a, const VV* csr_val, const VV* sell_val, const VX* x, Epi epi, cudaStream_t st) {
     constexpr int MB = sizeof(VV) == 4 ? 6 : 4;
-    const int warps = (a.sell_n_long - a.sell_n_vlong) + a.sell_slices;
-    const int blocks = a.sell_n_vlong + (warps + kThreads / 32 - 1) / (kThreads / 32);
+    constexpr int kWarps = kThreads / 32;
+    const int blocks = a.sell_n_vlong + (a.sell_n_long + kWarps - 1) / kWarps + sell_block_count(a);
     if (blocks <= 0) return;
     k_spmv_sell<VV, VX, Acc, Epi, MB><<<blocks, kThreads, 0, st>>>(
-        a.rows, a.sell_n_vlong, a.sell_n_long, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_off, a.sell_idx, sell_val,
-        x, epi);
+        a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
+        a.sell_n_long, a.sell_off, a.sell_idx, sell_val, x, epi);
     note_launch();
 }
 
