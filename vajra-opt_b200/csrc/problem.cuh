@@ -35,6 +35,7 @@ struct SellData {
     DeviceBuffer<double> val64;
     DeviceBuffer<float> val32;
     DeviceBuffer<int32_t> long_rows, vlong_rows;   // rows kept in CSR (row order)
+    DeviceBuffer<uint8_t> len;                     // row lengths, kSellLong for listed rows
 };
 
 struct Prepared {

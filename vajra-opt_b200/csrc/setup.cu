@@ -749,14 +749,16 @@ vajra_status order_by_degree(const DeviceLp& src, DeviceLp& dst, LpOrder& ord, c
 // ---------------------------------------------------------------------------------------
 // sliced ELL
 // ---------------------------------------------------------------------------------------
-// flags[r] = 1 for rows of kSellWidth..kSellCtaRow entries, 2 above; 0 for sliced rows.
+// is_long / is_vlong: rows of kSellWidth..kSellCtaRow entries / above (0 for sliced rows),
+// and the one-byte length the slices read (kSellLong for the listed rows).
 __global__ void k_sell_classify(int rows, const int64_t* __restrict__ ptr, uint8_t* __restrict__ is_long,
-                                uint8_t* __restrict__ is_vlong) {
+                                uint8_t* __restrict__ is_vlong, uint8_t* __restrict__ len8) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
     const int64_t len = ptr[r + 1] - ptr[r];
     is_long[r] = (len > kSellWidth && len <= kSellCtaRow) ? 1 : 0;
     is_vlong[r] = len > kSellCtaRow ? 1 : 0;
+    len8[r] = len > kSellWidth ? kSellLong : static_cast<uint8_t>(len);
 }
 
 // Slice s holds 32 x (its longest sliced row's length, rounded up to kSellPack) slots;
@@ -814,6 +816,7 @@ static vajra_status select_rows(int rows, const uint8_t* flags, DeviceBuffer<int
 vajra_status build_sell(CsrView& v, const double* val64, const float* val32, SellData& out, cudaStream_t st) {
     v.sell_off = nullptr;
     v.sell_idx = nullptr;
+    v.sell_len = nullptr;
     v.sell_long_rows = v.sell_vlong_rows = nullptr;
     v.sell_slices = v.sell_n_long = v.sell_n_vlong = 0;
     if (v.rows <= 0) return VAJRA_OK;
@@ -822,7 +825,9 @@ vajra_status build_sell(CsrView& v, const double* val64, const float* val32, Sel
         DeviceBuffer<uint8_t> is_long, is_vlong;
         VJ_TRY(is_long.alloc(static_cast<size_t>(v.rows)));
         VJ_TRY(is_vlong.alloc(static_cast<size_t>(v.rows)));
-        k_sell_classify<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, is_long.get(), is_vlong.get());
+        VJ_TRY(out.len.alloc(static_cast<size_t>(v.rows)));
+        k_sell_classify<<<grid_for(v.rows), kThreads, 0, st>>>(v.rows, v.ptr, is_long.get(), is_vlong.get(),
+                                                               out.len.get());
         VJ_LAUNCH_CHECK();
         note_launch(1);
         VJ_TRY(select_rows(v.rows, is_long.get(), out.long_rows, &n_long, st));
@@ -855,6 +860,7 @@ vajra_status build_sell(CsrView& v, const double* val64, const float* val32, Sel
     note_launch(1);
     v.sell_off = out.off.get();
     v.sell_idx = out.idx.get();
+    v.sell_len = out.len.get();
     v.sell_slices = slices;
     v.sell_long_rows = out.long_rows.get();
     v.sell_n_long = n_long;

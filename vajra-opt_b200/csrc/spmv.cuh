@@ -368,16 +368,20 @@ __device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict
 }
 
 // The rows of slice `sl` (one per lane) that are not listed as long.  No warp collectives.
+// sell_len[row]: the row's length, kSellLong for a listed row (one byte instead of two 8-byte
+// row pointers per row).
+constexpr uint8_t kSellLong = 0xFF;
+static_assert(kSellWidth < kSellLong, "row lengths of the slices must fit one byte below the marker");
+
 template <typename VV, typename VX, typename Acc, class Epi>
-__device__ __forceinline__ void sell_slice(int sl, int rows, const int64_t* __restrict__ ptr,
+__device__ __forceinline__ void sell_slice(int sl, int rows, const uint8_t* __restrict__ sell_len,
                                            const int64_t* __restrict__ sell_off, const int32_t* __restrict__ sell_idx,
                                            const VV* __restrict__ sell_val, const VX* __restrict__ x, const Epi& epi) {
     const int lane = threadIdx.x & 31;
     const int row = sl * 32 + lane;
     if (row >= rows) return;
-    const int64_t len64 = ptr[row + 1] - ptr[row];
-    if (len64 > kSellWidth) return;
-    const int len = static_cast<int>(len64);
+    const int len = __ldg(sell_len + row);
+    if (len == kSellLong) return;
     const PreOf<Epi> pre = epi_pre(epi, row, 0);
     Acc acc = Acc(0);
     if constexpr (kSellPack == 1) {
@@ -414,7 +418,8 @@ template <typename VV, typename VX, typename Acc, class Epi, int MB>
 __global__ void __launch_bounds__(kThreads, MB)
 k_spmv_sell(int rows, int slices, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
             const VV* __restrict__ val, const int32_t* __restrict__ vlong_rows, int n_vlong,
-            const int32_t* __restrict__ long_rows, int n_long, const int64_t* __restrict__ sell_off,
+            const int32_t* __restrict__ long_rows, int n_long, const uint8_t* __restrict__ sell_len,
+            const int64_t* __restrict__ sell_off,
             const int32_t* __restrict__ sell_idx, const VV* __restrict__ sell_val, const VX* __restrict__ x, Epi epi) {
     if (!epi.active()) return;
     int b = static_cast<int>(blockIdx.x);
@@ -444,7 +449,7 @@ k_spmv_sell(int rows, int slices, const int64_t* __restrict__ ptr, const int32_t
         return;
     }
     const int sl = (b - long_ctas) * kWarps + warp;
-    if (sl < slices) sell_slice<VV, VX, Acc>(sl, rows, ptr, sell_off, sell_idx, sell_val, x, epi);
+    if (sl < slices) sell_slice<VV, VX, Acc>(sl, rows, sell_len, sell_off, sell_idx, sell_val, x, epi);
 }
 
 // Host-side description of one SpMV operand (a CSR, possibly the stored transpose) and the
@@ -475,6 +480,7 @@ struct CsrView {
     // are passed to launch_sell by the caller.
     const int64_t* sell_off = nullptr;
     const int32_t* sell_idx = nullptr;
+    const uint8_t* sell_len = nullptr;
     int sell_slices = 0;
     const int32_t* sell_long_rows = nullptr;
     int sell_n_long = 0;
@@ -496,7 +502,7 @@ inline void launch_sell(const CsrView& a, const VV* csr_val, const VV* sell_val,
     if (blocks <= 0) return;
     k_spmv_sell<VV, VX, Acc, Epi, MB><<<blocks, kThreads, 0, st>>>(
         a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
-        a.sell_n_long, a.sell_off, a.sell_idx, sell_val, x, epi);
+        a.sell_n_long, a.sell_len, a.sell_off, a.sell_idx, sell_val, x, epi);
     note_launch();
 }
 
