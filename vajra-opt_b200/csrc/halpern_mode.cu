@@ -125,6 +125,9 @@ struct ControlParams {
     double pw_smoothing;
     int len;          // iterations in the chunk just finished
     int phase;
+    double gamma32;   // reflection of the FP32 phase once its KKT is below early_tol
+    double gamma64;   // reflection of the FP64 phase
+    double early_tol; // FP32 phase: above this KKT it reflects with gamma64 (its noise is far below)
     int mixed;        // 1 when an FP32 phase hands over to FP64
     int stall_checks; // FP32 stall window in checks (0 = no stall test; at most kHist - 1)
     int metric;       // restart metric: 0 weighted KKT, 1 fixed-point residual
@@ -188,9 +191,11 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
         }
         st->hist[hn % kHist] = rel;
         st->hist_n = hn + 1;
+        if (rel <= cp.early_tol) st->gamma_now = cp.gamma32;
         if (rel <= cp.switch_tol || stalled) {
             st->switch_flag = 1;
             st->phase = 1;
+            st->gamma_now = cp.gamma64;
             st->k_base = 0;
             st->kkt_start = wk;
             st->kkt_prev = wk;
@@ -394,15 +399,15 @@ void launch_iter(const CsrView& v, const T* csr_val, const T* sell_val, const T*
 }
 
 template <typename T>
-void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, const double* hw, double gamma, int kk,
+void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, const double* hw, int kk,
                        int write_cand, bool timed, cudaStream_t st) {
     if (timed) cudaEventRecordWithFlags(ph.ev[0], st, cudaEventRecordExternal);
     launch_iter<T>(at, ph.csc_val, ph.sell_val_at, ph.y.get(),
                    EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                 ph.xc.get(), ph.xprev.get(), S, hw, gamma, kk, ph.phase, write_cand}, st);
+                                 ph.xc.get(), ph.xprev.get(), S, hw, kk, ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[1], st, cudaEventRecordExternal);
     launch_iter<T>(a, ph.csr_val, ph.sell_val_a, ph.xb.get(),
-                   EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, gamma, kk,
+                   EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, kk,
                                ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[2], st, cudaEventRecordExternal);
 }
@@ -443,11 +448,11 @@ void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const 
 
 template <typename T>
 void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrView& a64, const CsrView& at64,
-                   const Prepared& p, const DeviceLp& lp, CheckBuffers& cb, HState* S, double gamma, int len,
+                   const Prepared& p, const DeviceLp& lp, CheckBuffers& cb, HState* S, int len,
                    ControlParams cp, bool capturing, cudaStream_t st) {
     // Event-record nodes (cudaEventRecordExternal) exist only inside a stream capture.
     for (int kk = 0; kk < len; ++kk)
-        enqueue_iteration(ph, a, at, S, cb.hw.get(), gamma, kk, kk == len - 1 ? 1 : 0, kk == 0 && capturing, st);
+        enqueue_iteration(ph, a, at, S, cb.hw.get(), kk, kk == len - 1 ? 1 : 0, kk == 0 && capturing, st);
     cp.len = len;
     cp.phase = ph.phase;
     enqueue_check(ph, a64, at64, p, lp, cb, S, cp, st);
@@ -459,7 +464,7 @@ void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrV
 // state whose phase is the tuned one; the iterates it scribbles on are re-initialised after.
 template <typename T>
 vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* tune_state, const CheckBuffers& cb,
-                                double gamma, cudaStream_t st) {
+                                cudaStream_t st) {
     const double* hw = cb.hw.get();
     k_halpern_weights<<<1, kThreads, 0, st>>>(tune_state, cb.hw_len, cb.hw.get());
     note_launch(1);
@@ -512,12 +517,12 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
     VJ_TRY(time_shapes(at, [&](const CsrView& t) {
         launch_iter<T>(t, ph.csc_val, ph.sell_val_at, ph.y.get(),
                        EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                     ph.xc.get(), ph.xprev.get(), tune_state, hw, gamma, 0, ph.phase, 0}, st);
+                                     ph.xc.get(), ph.xprev.get(), tune_state, hw, 0, ph.phase, 0}, st);
     }));
     VJ_TRY(time_shapes(a, [&](const CsrView& t) {
         launch_iter<T>(t, ph.csr_val, ph.sell_val_a, ph.xb.get(),
                        EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
-                                   tune_state, hw, gamma, 0, ph.phase, 0}, st);
+                                   tune_state, hw, 0, ph.phase, 0}, st);
     }));
     return VAJRA_OK;
 }
@@ -676,6 +681,11 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // A handle keeps its first tuning.
     const double gamma = o.reflection;
     const double gamma32 = (o.mixed_reflection > 0.0 && o.mixed_reflection <= 1.0) ? o.mixed_reflection : gamma;
+    // The FP32 phase averages its reflection only near its noise floor: far above it (more
+    // than kEarlyReflection x the hand-over tolerance) it takes the full FP64 step.
+    constexpr double kEarlyReflection = 10.0;
+    const double early_tol = kEarlyReflection * o.mixed_switch_tolerance;
+    init.gamma_now = gamma;   // the FP32 phase starts with the full step too
     CsrView a64 = p.a, at64 = p.at;
     CsrView a32 = p.a, at32 = p.at;
     // Below ~1M entries a solve is launch-bound and the timing runs would cost more than any
@@ -698,7 +708,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             tune.phase = 0;
             VJ_CUDA(cudaMemcpyAsync(dstate.get(), &tune, sizeof(tune), cudaMemcpyHostToDevice, st));
             init_iterates(p32, p, cb, st);
-            VJ_TRY(autotune_iteration<float>(p32, a32, at32, dstate.get(), cb, gamma, st));
+            VJ_TRY(autotune_iteration<float>(p32, a32, at32, dstate.get(), cb, st));
             h->tuned_a32 = a32.group;
             h->tuned_at32 = at32.group;
             h->tuned |= 1;
@@ -707,7 +717,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             tune.phase = 1;
             VJ_CUDA(cudaMemcpyAsync(dstate.get(), &tune, sizeof(tune), cudaMemcpyHostToDevice, st));
             init_iterates(p64, p, cb, st);
-            VJ_TRY(autotune_iteration<double>(p64, a64, at64, dstate.get(), cb, gamma, st));
+            VJ_TRY(autotune_iteration<double>(p64, a64, at64, dstate.get(), cb, st));
             h->tuned_a64 = a64.group;
             h->tuned_at64 = at64.group;
             h->tuned |= 2;
@@ -757,6 +767,9 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     ControlParams cp{};
     cp.tol = o.tolerance;
     cp.switch_tol = o.mixed_switch_tolerance;
+    cp.gamma32 = gamma32;
+    cp.gamma64 = gamma;
+    cp.early_tol = early_tol;
     cp.beta_sufficient = o.restart_sufficient;
     cp.beta_necessary = o.restart_necessary;
     cp.beta_artificial = o.restart_artificial;
@@ -780,7 +793,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 if (!ph.exec) {
                     const int64_t before = launch_count();
                     VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                    enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, ph.phase == 0 ? gamma32 : gamma, len, cp, true, st);
+                    enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, len, cp, true, st);
                     VJ_CUDA(cudaStreamEndCapture(st, &ph.graph));
                     VJ_CUDA(cudaGraphInstantiate(&ph.exec, ph.graph, 0));
                     ph.graph_kernels = launch_count() - before;
@@ -789,7 +802,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                 VJ_CUDA(cudaGraphLaunch(ph.exec, st));
                 note_launch(ph.graph_kernels);
             } else {
-                enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, ph.phase == 0 ? gamma32 : gamma, len, cp, false, st);
+                enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, len, cp, false, st);
                 VJ_LAUNCH_CHECK();
             }
             return VAJRA_OK;

@@ -11,6 +11,7 @@ constexpr int kHist = 32;
 struct HState {
     double omega, eta, tau, sigma;
     double inv_sigma;   // 1 / sigma, kept with sigma so the dual prox multiplies
+    double gamma_now;   // reflection coefficient of the running phase (set by the control)
     double kkt_start, kkt_prev;
     double rel_p, rel_d, rel_gap, rel_kkt, pobj, dobj;
     double bnorm, cnorm, offset_min;
@@ -45,15 +46,15 @@ struct EpiHPrimal {
     T* x; T* xb; T* xc; T* xprev;
     const HState* st;
     const double* hw;   // Halpern weights of this chunk: hw[2kk] = (k+1)/(k+2), hw[2kk+1] = 1/(k+2)
-    double gamma;
     int kk, phase, write_cand;
-    struct Pre { T xo, c, cl, cu, x0, tau, w1, w0; };
+    struct Pre { T xo, c, cl, cu, x0, tau, w1, w0, g; };
     __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
     __device__ Pre pre(int j) const {
         Pre p;
         p.w1 = static_cast<T>(__ldg(hw + 2 * kk));
         p.w0 = static_cast<T>(__ldg(hw + 2 * kk + 1));
         p.tau = static_cast<T>(__ldg(&st->tau));
+        p.g = static_cast<T>(__ldg(&st->gamma_now));
         p.xo = x[j];
         p.c = __ldg(c + j);
         p.cl = __ldg(cl + j);
@@ -63,7 +64,7 @@ struct EpiHPrimal {
     }
     template <typename Acc>
     __device__ void operator()(int j, Acc v, const Pre& p) const {
-        const T g = static_cast<T>(gamma);
+        const T g = p.g;
         T xp = p.xo - p.tau * (p.c + static_cast<T>(v));
         xp = xp < p.cl ? p.cl : (xp > p.cu ? p.cu : xp);
         xb[j] = xp + xp - p.xo;
@@ -80,9 +81,8 @@ struct EpiHDual {
     T* y; T* yc; T* yprev;
     const HState* st;
     const double* hw;   // Halpern weights of this chunk (as in EpiHPrimal)
-    double gamma;
     int kk, phase, write_cand;
-    struct Pre { T yo, rl, ru, y0, sigma, inv_sigma, w1, w0; };
+    struct Pre { T yo, rl, ru, y0, sigma, inv_sigma, w1, w0, g; };
     __device__ bool active() const { return st->stop == 0 && st->phase == phase; }
     __device__ Pre pre(int i) const {
         Pre p;
@@ -90,6 +90,7 @@ struct EpiHDual {
         p.w0 = static_cast<T>(__ldg(hw + 2 * kk + 1));
         p.sigma = static_cast<T>(__ldg(&st->sigma));
         p.inv_sigma = static_cast<T>(__ldg(&st->inv_sigma));
+        p.g = static_cast<T>(__ldg(&st->gamma_now));
         p.yo = y[i];
         p.rl = __ldg(rl + i);
         p.ru = __ldg(ru + i);
@@ -98,7 +99,7 @@ struct EpiHDual {
     }
     template <typename Acc>
     __device__ void operator()(int i, Acc w, const Pre& p) const {
-        const T g = static_cast<T>(gamma);
+        const T g = p.g;
         const T yh = p.yo + p.sigma * static_cast<T>(w);
         T q = yh * p.inv_sigma;
         q = q < p.rl ? p.rl : (q > p.ru ? p.ru : q);
