@@ -29,7 +29,7 @@ extern "C" {
 
 /* Layout version of the structs below.  A caller compiled against one version must not call
  * a library of another: compare with vajra_abi_version() before the first call. */
-#define VAJRA_ABI_VERSION 6
+#define VAJRA_ABI_VERSION 7
 
 typedef int32_t vajra_status;
 enum {
@@ -130,10 +130,11 @@ typedef struct vajra_opts {
                                    -3 sliced ELL (degree-ordered LPs; else the row-block
                                    kernel), 1..32 lanes per row (1, 2, 4, 8, 16, 32)        */
     int32_t spmv_shape_at;      /* the same for the A^T y SpMV                           */
-    double mixed_reflection;    /* MIXED: reflection coefficient of the FP32 phase (0.8); the
-                                   FP64 phase uses `reflection`.  Below 1 the reflected step is
-                                   averaged, which keeps FP32 rounding noise from building up
-                                   within a restart epoch                                 */
+    double mixed_reflection;    /* MIXED: reflection coefficient of the FP32 phase once its
+                                   relative KKT is within 10x of mixed_switch_tolerance (0.8);
+                                   above that, and in the FP64 phase, `reflection` applies.
+                                   Below 1 the reflected step is averaged, which keeps FP32
+                                   rounding noise from building up within a restart epoch  */
     int32_t degree_order;       /* HALPERN: renumber rows and columns by descending entry
                                    count on the device, so that the vector entries the SpMVs
                                    gather most often share cache lines; results come back in

@@ -16,7 +16,7 @@ _fp = C.POINTER(C.c_float)
 _i64p = C.POINTER(C.c_int64)
 _i32p = C.POINTER(C.c_int32)
 
-ABI_VERSION = 6   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
+ABI_VERSION = 7   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
 
 # vajra_status
 OK, ERR_INVALID_ARGUMENT, ERR_NO_DEVICE, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_WAIT_TIMEOUT, ERR_INTERNAL = range(7)
