@@ -505,11 +505,13 @@ def run(args, world, rank, local, dist):
     e2e = None
     if not args.no_e2e:
         barrier()
-        e2e_times = []
+        e2e_times, e2e_calls = [], []
         for _ in range(args.steps):
             t0 = time.perf_counter()
             r = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
             e2e_times.append(time.perf_counter() - t0)
+            e2e_calls.append({"wall_s": round(e2e_times[-1], 4), "library_total_s": round(r["total_time_sec"], 4),
+                              "device_s": round(r["device_time_sec"], 4), "setup_s": round(r["setup_time_sec"], 4)})
         barrier()
         h2d = 8 * (lp.num_cols + 1) + 12 * lp.nnz + 8 * (3 * lp.num_cols + 2 * lp.num_rows)
         d2h = 8 * (2 * lp.num_cols + 2 * lp.num_rows)
@@ -517,7 +519,8 @@ def run(args, world, rank, local, dist):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "status": r["status_name"], "rel_kkt": r["rel_kkt"],
                "last_call_breakdown_s": {k: r[k] for k in ("upload_time_sec", "setup_time_sec", "iteration_time_sec",
-                                                           "download_time_sec", "total_time_sec", "device_time_sec")}}
+                                                           "download_time_sec", "total_time_sec", "device_time_sec")},
+               "calls": e2e_calls}
 
     # ---- roofline of the dominant iteration kernel ----------------------------------
     peak, peak_kind = load_peaks()
