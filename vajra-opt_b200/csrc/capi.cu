@@ -4,6 +4,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -34,6 +36,70 @@ vajra_status cuda_status(cudaError_t e, const char* what, const char* file, int 
     if (e == cudaErrorMemoryAllocation) return VAJRA_ERR_OUT_OF_MEMORY;
     if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return VAJRA_ERR_NO_DEVICE;
     return VAJRA_ERR_CUDA;
+}
+
+// ----- device block cache (common.cuh) -------------------------------------------------
+namespace {
+struct BlockCache {
+    std::mutex mu;
+    std::map<std::pair<int, size_t>, std::vector<void*>> free_blocks;
+    size_t cached_bytes = 0;
+};
+BlockCache& block_cache() {
+    static BlockCache* c = new BlockCache();   // never destroyed: blocks live until exit
+    return *c;
+}
+// Size classes: powers of two up to 1 MiB, whole MiB above.
+size_t size_class(size_t bytes) {
+    constexpr size_t kMiB = size_t(1) << 20;
+    if (bytes >= kMiB) return (bytes + kMiB - 1) / kMiB * kMiB;
+    size_t c = 512;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+}  // namespace
+
+size_t block_cache_limit() { return size_t(16) << 30; }
+
+cudaError_t cached_alloc(void** p, size_t bytes, int* device) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    *device = dev;
+    const size_t cls = size_class(bytes);
+    {
+        BlockCache& c = block_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.free_blocks.find({dev, cls});
+        if (it != c.free_blocks.end() && !it->second.empty()) {
+            *p = it->second.back();
+            it->second.pop_back();
+            c.cached_bytes -= cls;
+            return cudaSuccess;
+        }
+    }
+    return cudaMalloc(p, cls);
+}
+
+void cached_release(void* p, size_t bytes, int device) {
+    const size_t cls = size_class(bytes);
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) return;
+    if (cur != device) cudaSetDevice(device);
+    // Nothing still queued on the device may touch the block once it is handed out again.
+    const bool idle = cudaDeviceSynchronize() == cudaSuccess;
+    bool kept = false;
+    if (idle) {
+        BlockCache& c = block_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (c.cached_bytes + cls <= block_cache_limit()) {
+            c.free_blocks[{device, cls}].push_back(p);
+            c.cached_bytes += cls;
+            kept = true;
+        }
+    }
+    if (!kept) cudaFree(p);
+    if (cur != device) cudaSetDevice(cur);
 }
 
 void copy_out_vector(double* dst, const double* dev, int count, cudaStream_t st) {

@@ -48,7 +48,18 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
     return static_cast<unsigned>(g);
 }
 
-// Owning device allocation.  Moves only; frees on destruction.
+// Device blocks go through a process-wide cache keyed by (device, size class): a released
+// block waits for its device to finish all work (the ordering cudaFree gives) and is kept for
+// the next request of its size class on that device, which then needs no driver call.  A
+// solve allocates and releases the same few dozen buffers every run; on shared machines those
+// driver calls were where the occasional multi-second host stalls of a solve showed up.  At
+// most block_cache_limit() bytes are kept; beyond that blocks are freed.  Cached blocks keep
+// their old contents (so does fresh cudaMalloc memory: nothing may assume zeros).
+cudaError_t cached_alloc(void** p, size_t bytes, int* device);
+void cached_release(void* p, size_t bytes, int device);
+size_t block_cache_limit();
+
+// Owning device allocation.  Moves only; releases on destruction.
 template <typename T>
 class DeviceBuffer {
 public:
@@ -56,9 +67,9 @@ public:
     ~DeviceBuffer() { reset(); }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+    DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), dev_(o.dev_) { o.p_ = nullptr; o.n_ = 0; }
     DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
-        if (this != &o) { reset(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+        if (this != &o) { reset(); p_ = o.p_; n_ = o.n_; dev_ = o.dev_; o.p_ = nullptr; o.n_ = 0; }
         return *this;
     }
     // Every allocation carries kPad spare elements, so 128-bit vector loads of the last
@@ -67,13 +78,15 @@ public:
     vajra_status alloc(size_t n) {
         reset();
         if (n == 0) n = 1;   // keep a valid pointer for empty extents
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p_), (n + kPad) * sizeof(T));
+        void* p = nullptr;
+        cudaError_t e = cached_alloc(&p, (n + kPad) * sizeof(T), &dev_);
         if (e != cudaSuccess) { p_ = nullptr; return cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
+        p_ = static_cast<T*>(p);
         n_ = n;
         return VAJRA_OK;
     }
     void reset() noexcept {
-        if (p_) cudaFree(p_);
+        if (p_) cached_release(p_, (n_ + kPad) * sizeof(T), dev_);
         p_ = nullptr;
         n_ = 0;
     }
@@ -83,6 +96,7 @@ public:
 private:
     T* p_ = nullptr;
     size_t n_ = 0;
+    int dev_ = 0;
 };
 
 // ---------------------------------------------------------------------------------------
