@@ -3,15 +3,22 @@
 // which is where the dual / primal prox, Halpern and KKT work is fused, so a row sum never
 // makes a round trip through HBM.
 //
-// Two families:
-//   k_spmv_seq  one thread per row, products added in storage order with explicit _rn
-//               intrinsics (no FMA contraction).  Over a CSR whose rows are sorted by column
-//               this reproduces the reference's CSC scatter SpMV (src/linalg/sparse.cpp:196-217)
-//               and in-order dot (:219-238) bit for bit, including the |x_j| <= 1e-11 skip.
-//   k_spmv_vec  G lanes per row (G = 1..32, picked per matrix by the autotuner), coalesced
-//               strided loads with streaming (evict-first) cache hints for the matrix and
-//               cached gathers for the dense vector, xor-butterfly reduction (deterministic),
-//               and trailing CTAs that take the rows longer than `long_len` one CTA per row.
+// Kernel families:
+//   k_spmv_seq       one thread per row, products added in storage order with explicit _rn
+//                    intrinsics (no FMA contraction).  Over a CSR whose rows are sorted by
+//                    column this reproduces the reference's CSC scatter SpMV
+//                    (src/linalg/sparse.cpp:196-217) and in-order dot (:219-238) bit for bit,
+//                    including the |x_j| <= 1e-11 skip.
+//   k_spmv_vec       G lanes per row (G = 1..32), coalesced strided loads with streaming
+//                    (evict-first) cache hints for the matrix and cached gathers for the dense
+//                    vector, xor-butterfly reduction (deterministic), and trailing CTAs that
+//                    take the rows longer than `long_len` one CTA per row.
+//   k_spmv_rowblock  blocks of consecutive rows holding ~2048 entries, products staged in
+//                    shared memory, then summed per row (one or two load groups per thread).
+//   k_spmv_sell      sliced ELL: 32 rows a slice, a thread per row, the row's entries in pairs
+//                    laid out so that every load is coalesced across the warp (the fastest
+//                    form on rows numbered by length, as the degree-ordered LP has them).
+// The autotuner of each solver picks the family and shape per matrix and precision.
 #pragma once
 
 #include "common.cuh"
