@@ -270,10 +270,23 @@ vajra_status vajra_probe_device(int32_t device, vajra_device_info* info) {
         std::snprintf(info->device_name, sizeof(info->device_name), "None (No CUDA devices found)");
         return VAJRA_ERR_NO_DEVICE;
     }
+    // The static properties are read once per device (cudaGetDeviceProperties takes
+    // milliseconds and every solve asks twice); free memory below stays live.
+    static std::mutex props_mu;
+    static std::map<int, cudaDeviceProp> props_cache;
     cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
-        std::snprintf(info->device_name, sizeof(info->device_name), "Error querying CUDA device");
-        return VAJRA_ERR_CUDA;
+    {
+        std::lock_guard<std::mutex> lock(props_mu);
+        auto it = props_cache.find(device);
+        if (it == props_cache.end()) {
+            if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+                std::snprintf(info->device_name, sizeof(info->device_name), "Error querying CUDA device");
+                return VAJRA_ERR_CUDA;
+            }
+            props_cache.emplace(device, prop);
+        } else {
+            prop = it->second;
+        }
     }
     info->available = 1;
     std::snprintf(info->device_name, sizeof(info->device_name), "%s", prop.name);
