@@ -13,7 +13,9 @@
 // with deterministic block partials and one control CTA that forms the relative KKT on the
 // original problem, the primal-weighted KKT for restarts (sufficient 0.2 / necessary 0.8 +
 // no progress / artificial 0.36 of total), the primal-weight update at restarts, and -- in
-// mixed precision -- the hand-over from the FP32 phase to the FP64 polish.
+// mixed precision -- the FP32 phase's reflection coefficient and its hand-over to the FP64
+// polish.  Large LPs are first renumbered by row / column length (degree ordering) and get
+// sliced-ELL copies of both matrices; results go back to the caller's numbering.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -459,9 +461,9 @@ void enqueue_chunk(Phase<T>& ph, const CsrView& a, const CsrView& at, const CsrV
 }
 
 // Times every launch shape (row-block kernel with one or two load groups, 1..32 lanes per
-// row) of both iteration kernels
-// with their real epilogues and keeps the fastest per matrix.  `tune_state` is a scratch
-// state whose phase is the tuned one; the iterates it scribbles on are re-initialised after.
+// row, and sliced ELL where the set-up built it) of both iteration kernels with their real
+// epilogues and keeps the fastest per matrix.  `tune_state` is a scratch state whose phase is
+// the tuned one; the iterates it scribbles on are re-initialised after.
 template <typename T>
 vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* tune_state, const CheckBuffers& cb,
                                 cudaStream_t st) {
