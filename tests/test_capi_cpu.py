@@ -39,6 +39,9 @@ def test_default_opts():
     o = V.default_opts()
     assert o.algorithm == V.ALGO_HALPERN and o.precision == V.PREC_MIXED
     assert o.tolerance == 1e-6 and o.check_frequency == 64 and o.enable_scaling == 1
+    assert o.mixed_switch_tolerance == 2e-6 and o.mixed_reflection == 0.8 and o.reflection == 1.0
+    assert o.degree_order == 0 and o.spmv_shape_a == 0 and o.spmv_shape_at == 0 and o.autotune == 1
+    assert o.restart_sufficient == 0.2 and o.restart_necessary == 0.8 and o.restart_artificial == 0.36
     with pytest.raises(KeyError):
         V.default_opts(no_such_option=1)
 
