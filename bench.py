@@ -68,16 +68,28 @@ def parse():
     ap.add_argument("--study", choices=["small", "flow", "adjoint"], default=None,
                     help="one JSON line for another workload: small = 2000x5000 planted LP, flow = min-cost "
                          "flow 200k nodes x 1.5M arcs, adjoint = 256 x (1000x3000) unrolled-PDHG gradients vs FD")
+    ap.add_argument("--no-batch-sharded", action="store_true",
+                    help="N > 1: skip the sharded batched solve reported beside the replica line")
+    ap.add_argument("--plumbing-check", action="store_true",
+                    help="rank plumbing only (no solve, gloo without a GPU): spawn, barrier, max over ranks")
     ap.add_argument("--batch-sequential", type=int, default=-1,
                     help="how many of the LPs to time sequentially (default all; the rate is per solve)")
     return ap.parse_args()
 
 
 def run_batch_bench(args, world=1, rank=0, dist=None):
+    line = batch_line(args, world, rank, dist)
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def batch_line(args, world=1, rank=0, dist=None, sequential=True):
     """Batched block-diagonal solve vs sequential plain FP64 solves of the same LPs.
 
     With N > 1 ranks the instances are sharded by nnz (no collective on the data path; one
-    gather of per-instance summaries at the end) and the wall time is the slowest rank's."""
+    gather of per-instance summaries at the end) and the wall time is the slowest rank's.
+    Returns the JSON line on rank 0, None on the other ranks."""
     import numpy as np
     import torch
     import vajra_pdhg as V
@@ -85,7 +97,7 @@ def run_batch_bench(args, world=1, rank=0, dist=None):
     from vajra_pdhg import workloads as W
     from vajra_pdhg.kkt import relative_kkt
     dev = torch.device("cuda", torch.cuda.current_device())
-    lps = W.batch(args.batch, seed=3)
+    lps = W.batch(args.batch if args.batch > 0 else 512, seed=3)
     nnz = sum(lp.nnz for lp in lps)
     shard = S.partition_by_nnz([lp.nnz for lp in lps], world)[rank]
     for _ in range(max(1, args.warmup)):
@@ -102,7 +114,7 @@ def run_batch_bench(args, world=1, rank=0, dist=None):
     worst_kkt = S.max_over_ranks(max((relative_kkt(lps[i], r["x"], r["y"])["rel_kkt"] for i, r in zip(mine, res)),
                                      default=0.0), dist, dev)
     if rank != 0:
-        return 0
+        return None
     iters = [s["iterations"] for s in summaries]
     line = {"metric": "batched solves/s vs sequential plain FP64 solves (rel KKT 1e-6 each)",
             "value": len(lps) / batch_wall, "unit": "solves/s", "higher_is_better": True, "n_gpus": world,
@@ -116,7 +128,7 @@ def run_batch_bench(args, world=1, rank=0, dist=None):
             "config": {"workload": f"{len(lps)} LPs, m log-uniform on [100, 20000], n = round(U[2,3] m), "
                                    f"nnz per column U{{4..12}}, planted optima, seed 3",
                        "parallelism": f"instances sharded by nnz over {world} rank(s)"}}
-    if world == 1:
+    if world == 1 and sequential:
         nseq = len(lps) if args.batch_sequential < 0 else min(args.batch_sequential, len(lps))
         V.solve(lps[0], precision=V.PREC_FP64)
         seq_times, seq_ok = [], 0
@@ -129,8 +141,7 @@ def run_batch_bench(args, world=1, rank=0, dist=None):
         line["sequential"] = {"timed": nseq, "total_s_for_all": seq_total, "solves_per_s": len(lps) / seq_total,
                               "optimal": seq_ok}
         line["speedup"] = seq_total / batch_wall
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def run_study(args, local=0):
@@ -340,10 +351,45 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl"
+        if args.plumbing_check and not torch.cuda.is_available():
+            backend = "gloo"                 # the plumbing check on a host without GPUs
+        else:
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
+
+
+def free_port() -> int:
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_ranks(n: int) -> int:
+    """`--gpus N` without a launcher around it: start N ranks (one process per GPU) under
+    torch.distributed.run on 127.0.0.1, each running this script with the same arguments."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={free_port()}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
+def plumbing_check(args, world, rank, dist):
+    """Every rank contributes a stand-in step time (rank-dependent), the ranks meet at a
+    barrier and rank 0 prints the maximum over ranks with the rank count: the launcher,
+    process group and reduction of the timed runs, without a device."""
+    import torch
+    from vajra_pdhg import sharding as S
+    if dist:
+        dist.barrier()
+    value = S.max_over_ranks(1.0 + 0.25 * rank, dist, torch.device("cpu") if not torch.cuda.is_available()
+                             else torch.device("cuda", torch.cuda.current_device()))
+    ranks = S.gather_objects(rank, dist)
+    if rank == 0:
+        print(json.dumps({"plumbing_check": True, "n_gpus": world, "ranks": ranks, "value": value}))
+    return 0
 
 
 def pinned_copy(lp):
@@ -389,8 +435,12 @@ def workload_config(args, lp):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
     world, rank, local, dist = dist_setup(args)
     try:
+        if args.plumbing_check:
+            return plumbing_check(args, world, rank, dist)
         return run(args, world, rank, local, dist)
     finally:
         if dist is not None and dist.is_initialized():
@@ -429,6 +479,9 @@ def run(args, world, rank, local, dist):
                                            f"algorithm stalls near 1e-4 and never reaches 1e-6)",
                                  "per_iteration_s": per_iter, "setup_s": setup,
                                  "status_after_sample": samples[-1]["status"]},
+                "value_kind": f"estimate: measured set-up + measured per-iteration time x {iters_needed} "
+                              f"iterations; the measured quantity is per_iteration_s",
+                "per_iteration_s": per_iter,
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -442,7 +495,7 @@ def run(args, world, rank, local, dist):
     if args.study:
         return run_study(args, local) if rank == 0 else 0
     torch.cuda.set_device(local)
-    lp = W.random_large(args.rows, args.cols, seed=args.seed + rank)
+    lp = W.random_large(args.rows, args.cols, seed=args.seed)      # the same LP on every rank (replicas)
     if args.profile_iters > 0:
         prec = V.PREC_MIXED if args.profile_precision == "mixed" else V.PREC_FP64
         shapes = {}
@@ -457,6 +510,15 @@ def run(args, world, rank, local, dist):
                           "primal_bytes": r["primal_kernel_bytes"], "dual_bytes": r["dual_kernel_bytes"]}))
         return 0
     plp = pinned_copy(lp)
+    # The first end-to-end call of a fresh process: it pays the SpMV autotuning (~0.4 s on this
+    # LP) and the first device allocations, which every later call finds cached.
+    cold = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc0 = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
+        cold = {"wall_s": round(time.perf_counter() - t0, 4), "setup_s": round(rc0["setup_time_sec"], 4),
+                "status": rc0["status_name"]}
 
     def barrier():
         if dist:
@@ -489,6 +551,15 @@ def run(args, world, rank, local, dist):
     ok = all(r["status_name"] == "OPTIMAL" for r in results)
     host_kkt = relative_kkt(lp, last["x"], last["y"])
 
+    # ---- N > 1: the batched workload sharded over the ranks (the path that shards) -----
+    batch_sharded = None
+    if world > 1 and not args.no_batch_sharded:
+        bl = batch_line(args, world, rank, dist, sequential=False)
+        if bl is not None:
+            batch_sharded = {"solves_per_s": bl["value"], "count": bl["batch"]["count"],
+                             "wall_s": bl["batch"]["wall_s"], "optimal": bl["batch"]["optimal"],
+                             "worst_host_rel_kkt": bl["batch"]["worst_host_rel_kkt"], "scaling": "strong"}
+
     # ---- plain FP64 form --------------------------------------------------------------
     fp64 = None
     if args.fp64_steps > 0:
@@ -505,22 +576,21 @@ def run(args, world, rank, local, dist):
     e2e = None
     if not args.no_e2e:
         barrier()
-        e2e_times, e2e_calls = [], []
+        e2e_times = []
         for _ in range(args.steps):
             t0 = time.perf_counter()
             r = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
             e2e_times.append(time.perf_counter() - t0)
-            e2e_calls.append({"wall_s": round(e2e_times[-1], 4), "library_total_s": round(r["total_time_sec"], 4),
-                              "device_s": round(r["device_time_sec"], 4), "setup_s": round(r["setup_time_sec"], 4)})
         barrier()
         h2d = 8 * (lp.num_cols + 1) + 12 * lp.nnz + 8 * (3 * lp.num_cols + 2 * lp.num_rows)
         d2h = 8 * (2 * lp.num_cols + 2 * lp.num_rows)
         e2e = {"value": max_over_ranks(statistics.mean(e2e_times)), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "status": r["status_name"], "rel_kkt": r["rel_kkt"],
-               "last_call_breakdown_s": {k: r[k] for k in ("upload_time_sec", "setup_time_sec", "iteration_time_sec",
-                                                           "download_time_sec", "total_time_sec", "device_time_sec")},
-               "calls": e2e_calls}
+               "calls_min_max_s": [round(min(e2e_times), 4), round(max(e2e_times), 4)],
+               "last_setup_s": round(r["setup_time_sec"], 4), "last_device_s": round(r["device_time_sec"], 4)}
+        if cold is not None:
+            e2e["cold_first_call"] = cold
 
     # ---- roofline of the dominant iteration kernel ----------------------------------
     peak, peak_kind = load_peaks()
@@ -535,9 +605,9 @@ def run(args, world, rank, local, dist):
                 if peak_kind == "measured" else "fallback 6650 GB/s",
                 "traffic": (traffic or {}).get("dominant_bytes_per_launch"),
                 "bytes_per_launch": byts, "avg_launch_us": us, "samples": last["kernel_samples"],
-                "per_kernel": {k: {"avg_us": v[0], "algorithmic_bytes": v[1],
-                                   "gbs": (v[1] / (v[0] * 1e-6) / 1e9) if v[0] > 0 else None}
-                               for k, v in kern.items()}}
+                "per_kernel_us_gbs": {("primal" if k.startswith("primal") else "dual"):
+                                      [round(v[0], 2), round(v[1] / (v[0] * 1e-6) / 1e9, 1) if v[0] > 0 else None]
+                                      for k, v in kern.items()}}
 
     # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
     cpu = None
@@ -566,16 +636,21 @@ def run(args, world, rank, local, dist):
                 "warmup": args.warmup, "ms_per_step": 1e3 * value, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32 iterations + f64 checks/polish",
                 "data": "synthetic", "config": workload_config(args, lp),
-                "correct": {"all_optimal": ok, "device_rel_kkt": last["rel_kkt"], "host_rel_kkt": host_kkt["rel_kkt"],
-                            "objective": last["objective_value"], "planted_objective": lp.planted_objective,
-                            "objective_rel_err_vs_planted": abs(last["objective_value"] - lp.planted_objective) /
-                            (1 + abs(lp.planted_objective)),
-                            "iterations": last["iterations"], "fp32_iterations": last["fp32_iterations"],
-                            "fp64_iterations": last["fp64_iterations"], "restarts": last["restart_count"]},
-                "fp64_plain": fp64,
-                "speedup_vs_fp64": (fp64["value"] / value) if fp64 else None,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
-                "spmv_groups": {"A": last["spmv_group_a"], "A^T": last["spmv_group_at"]}}
+                "spmv_groups": {"A": last["spmv_group_a"], "A^T": last["spmv_group_at"]},
+                "per_iteration_s": value / max(1, last["iterations"])}
+        if batch_sharded is not None:
+            line["batch_sharded"] = batch_sharded
+        # last, so that a reader keeping only the end of the line keeps them
+        line["fp64_plain"] = fp64
+        line["correct"] = {"all_optimal": ok, "device_rel_kkt": last["rel_kkt"], "host_rel_kkt": host_kkt["rel_kkt"],
+                           "objective_rel_err_vs_planted": abs(last["objective_value"] - lp.planted_objective) /
+                           (1 + abs(lp.planted_objective)),
+                           "fp64_vs_mixed_objective_rel": (abs(fp64["objective"] - last["objective_value"]) /
+                                                           (1 + abs(last["objective_value"]))) if fp64 else None,
+                           "iterations": last["iterations"], "fp32_iterations": last["fp32_iterations"],
+                           "fp64_iterations": last["fp64_iterations"], "restarts": last["restart_count"]}
+        line["speedup_vs_fp64"] = (fp64["value"] / value) if fp64 else None
         print(json.dumps(line))
     if dist:
         dist.barrier()

@@ -38,7 +38,7 @@ enum {
     VAJRA_ERR_NO_DEVICE = 2,
     VAJRA_ERR_CUDA = 3,
     VAJRA_ERR_OUT_OF_MEMORY = 4,
-    VAJRA_ERR_WAIT_TIMEOUT = 5,  /* a bounded device-side wait gave up (batched kernel) */
+    VAJRA_ERR_WAIT_TIMEOUT = 5,  /* reserved: no entry point waits on the device today      */
     VAJRA_ERR_INTERNAL = 6
 };
 
@@ -256,6 +256,26 @@ vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const va
 vajra_status vajra_pdhg_run(vajra_pdhg* handle, vajra_result* result);
 vajra_status vajra_pdhg_destroy(vajra_pdhg* handle);
 
+/* The device set-up's scaling of one LP, exported so that it can be checked against the
+ * reference's host scaling: Ruiz equilibration exactly as RuizScaler::compute_and_scale
+ * (src/linalg/scaling.cpp:7-153; opts->ruiz_iterations passes, tolerance 0.05), then -- with
+ * opts->pock_chambolle -- the Pock-Chambolle diagonal preconditioner of
+ * PockChambollePreconditioner::compute (scaling.cpp:179-220, alpha = 1) applied symmetrically:
+ * A <- diag(sqrt(d_row)) A diag(sqrt(d_col)) on the Ruiz-scaled A, which is the same saddle
+ * problem as PDHG with the step matrices diag(d_col), diag(d_row).  Outputs (host, any may be
+ * NULL): the cumulative row_scale[m] and col_scale[n], the scaled values[nnz] in CSC order, the
+ * scaled c[n] (negated for maximisation), col_lower/col_upper[n] and row_lower/row_upper[m]. */
+vajra_status vajra_scale_lp(const vajra_lp* lp, const vajra_opts* opts, double* row_scale, double* col_scale,
+                            double* values, double* c, double* col_lower, double* col_upper, double* row_lower,
+                            double* row_upper);
+
+/* The library keeps released device blocks in a per-device cache (up to 16 GiB, or
+ * VAJRA_BLOCK_CACHE_MB megabytes read at the first allocation) so that repeated solves reuse
+ * them without driver calls.  This returns every cached block of `device` (every device for a
+ * negative ordinal) to the driver and reports the bytes freed; blocks in use by a live solve or
+ * handle are not touched.  No counterpart in the reference (it allocates and frees per solve). */
+int64_t vajra_release_cached_memory(int32_t device);
+
 /* ---- differentiation: adjoint of the unrolled PDHG map ---------------------------
  * No counterpart in the reference (it has no derivatives); the forward map is the plain
  * PDHG iteration of src/solvers/pdhg/pdhg.cpp:196-241 (primal first, fixed steps
@@ -322,7 +342,8 @@ vajra_status vajra_primal_prox_f64(int32_t cols, double tau, const double* aty, 
                                    const double* col_lower, const double* col_upper, double* x,
                                    double* x_bar, void* stream);
 /* compute_diagnostics_device_kernel (spmv_kernels.cuh:210-278); out is a device pointer.
- * Deterministic block reductions instead of the reference's CAS atomics. */
+ * A grid of CTAs with a deterministic two-stage reduction instead of the reference's CAS
+ * atomics; the block partials come from the stream-ordered pool (cudaMallocAsync) on `stream`. */
 vajra_status vajra_device_diagnostics_f64(int32_t rows, int32_t cols, const double* ax,
                                           const double* row_lower, const double* row_upper,
                                           const double* aty, const double* c, const double* x,
@@ -349,8 +370,11 @@ vajra_status vajra_pdhg_step_f64(int32_t rows, int32_t cols,
  * objective (minimisation form, offset included).
  * No counterpart in the reference.  It allocates nothing, for callers that cannot call
  * cudaMalloc: its scratch is a fixed 2 MiB device array inside the library, which limits
- * rows and columns to 8,388,608 each (larger sizes return VAJRA_ERR_INVALID_ARGUMENT).  The
- * first call on a device looks up that array's address; make it before any stream capture.
+ * rows and columns to 8,388,608 each (larger sizes return VAJRA_ERR_INVALID_ARGUMENT).  Each
+ * call outside a stream capture looks up that array's address on the current device; a call
+ * inside a capture reuses the address the last such call found, so make the first call on a
+ * device -- and the first after a cudaDeviceReset or primary-context reset -- outside any
+ * capture.  An LP without rows (rows = 0) is accepted; its row-side pointers may then be NULL.
  * Nothing has to start at zero: each call writes every partial sum it later reads.  All calls
  * on a device share the array: calls that overlap on the GPU race. */
 vajra_status vajra_relative_kkt_noalloc_f64(int32_t rows, int32_t cols, const int64_t* row_ptr,

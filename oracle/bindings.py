@@ -142,6 +142,7 @@ def ref():
         lib.ref_spectral_norm.restype = C.c_double
         lib.ref_spectral_norm.argtypes = [C.POINTER(LpStruct), C.c_int32, C.c_double]
         lib.ref_ruiz.argtypes = [C.POINTER(LpStruct), C.c_int32, C.c_double] + [_dp] * 8
+        lib.ref_pock_chambolle.argtypes = [C.POINTER(LpStruct), C.c_double, _dp, _dp]
         lib.ref_csc_multiply.argtypes = [C.POINTER(LpStruct), _dp, _dp]
         lib.ref_csc_multiply_transpose.argtypes = [C.POINTER(LpStruct), _dp, _dp]
         lib.ref_verify.argtypes = [C.POINTER(LpStruct), _dp, _dp, C.c_double, C.c_int32, C.c_double,
@@ -240,6 +241,15 @@ def ref_ruiz(lp, max_iters=10, tol=0.05):
     ref().ref_ruiz(C.byref(h.s), max_iters, tol, *[_ptr(a, _dp) for a in (vals, c, rl, ru, cl, cu, rs, cs)])
     return dict(values=vals, c=c, row_lower=rl, row_upper=ru, col_lower=cl, col_upper=cu,
                 row_scale=rs, col_scale=cs)
+
+
+def ref_pock_chambolle(lp, alpha=1.0):
+    """The reference's PockChambollePreconditioner::compute (src/linalg/scaling.cpp:179-220) on
+    lp's matrix: d_row = 1 / sum_j |a_ij|^(2 - alpha), d_col = 1 / sum_i |a_ij|^alpha."""
+    h = HostLp(lp)
+    d_row, d_col = np.zeros(lp.num_rows), np.zeros(lp.num_cols)
+    ref().ref_pock_chambolle(C.byref(h.s), alpha, _ptr(d_row, _dp), _ptr(d_col, _dp))
+    return d_row, d_col
 
 
 def port_device_diagnostics(ax, rl, ru, aty, c, x, y, cl, cu):

@@ -10,6 +10,7 @@
 //                          or indus::solve (status guard)         src/engine/model.cpp:376-667
 //   ref_spectral_norm   -> indus::pdhg::estimate_spectral_norm    src/solvers/pdhg/pdhg.cpp:11-56
 //   ref_ruiz            -> indus::la::RuizScaler::compute_and_scale src/linalg/scaling.cpp:7-153
+//   ref_pock_chambolle  -> indus::la::PockChambollePreconditioner::compute src/linalg/scaling.cpp:179-220
 //   ref_csc_multiply(_transpose) -> SparseMatrixCSC::multiply(_transpose) src/linalg/sparse.cpp:196-238
 //   ref_verify          -> indus::verifier::verify_solution       src/engine/verifier.cpp:25-330
 //
@@ -204,6 +205,16 @@ int ref_ruiz(const ref_lp* lp, int32_t max_iters, double tol,
     copy_out(sf.row_scale, row_scale_out);
     copy_out(sf.col_scale, col_scale_out);
     return sf.is_scaled ? 1 : 0;
+}
+
+// Pock-Chambolle diagonal preconditioners of the LP's matrix as given (the caller passes the
+// Ruiz-scaled values to compose the two, as the device set-up does): d_row[m], d_col[n].
+void ref_pock_chambolle(const ref_lp* lp, double alpha, double* d_row_out, double* d_col_out) {
+    indus::Model model = make_model(lp);
+    std::vector<double> d_row, d_col;
+    indus::la::PockChambollePreconditioner::compute(model.A, d_row, d_col, alpha);
+    copy_out(d_row, d_row_out);
+    copy_out(d_col, d_col_out);
 }
 
 void ref_csc_multiply(const ref_lp* lp, const double* x, double* y) {

@@ -142,3 +142,24 @@ def test_spmv_bit_identical_to_oracle_random(cuda, seed):
     A = lp.to_scipy_csc().astype(np.float32)
     ref32 = A.T @ y.astype(np.float32)
     np.testing.assert_allclose(host(out32), ref32, rtol=1e-5, atol=1e-5)
+
+
+def test_device_diagnostics_many_ctas_match_the_oracle(cuda):
+    """1.5M columns and 0.7M rows (a grid of CTAs and the two-stage reduction): maxima exact,
+    the objective sum to rounding, against the oracle's sequential evaluation."""
+    rng = np.random.default_rng(17)
+    m, n = 700_000, 1_500_000
+    rl = rng.standard_normal(m); ru = rl + rng.random(m); ru[::7] = 1e20; rl[::5] = -1e20
+    ax = rng.standard_normal(m) * 2
+    cl = np.where(rng.random(n) < 0.9, 0.0, -1e20); cu = np.where(rng.random(n) < 0.8, 10.0, 1e20)
+    x = rng.random(n) * 11 - 0.5
+    c, aty, y = rng.standard_normal(n), rng.standard_normal(n), rng.standard_normal(m)
+    arrays = (ax, rl, ru, aty, c, x, y, cl, cu)
+    keep = [dev(a, np.float64) for a in arrays]
+    out = dev(np.zeros(6))
+    assert _capi.lib().vajra_device_diagnostics_f64(m, n, *[p(t) for t in keep], p(out), None) == 0
+    d = _capi.VajraDeviceDiagnostics.from_buffer_copy(host(out).tobytes())
+    o = B.port_device_diagnostics(*arrays)
+    assert d.primal_residual == o["primal_residual"] and d.dual_residual == o["dual_residual"]
+    assert d.numerical_error == o["numerical_error"] == 0
+    assert abs(d.objective - o["objective"]) <= 1e-9 * (1 + abs(o["objective"]))

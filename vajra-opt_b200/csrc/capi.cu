@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -59,7 +60,40 @@ size_t size_class(size_t bytes) {
 }
 }  // namespace
 
-size_t block_cache_limit() { return size_t(16) << 30; }
+// 16 GiB unless VAJRA_BLOCK_CACHE_MB says otherwise (0 keeps no blocks: every release frees).
+size_t block_cache_limit() {
+    static const size_t limit = [] {
+        const char* v = std::getenv("VAJRA_BLOCK_CACHE_MB");
+        if (v && *v) {
+            char* end = nullptr;
+            const unsigned long long mb = std::strtoull(v, &end, 10);
+            if (end && *end == '\0') return static_cast<size_t>(mb) << 20;
+        }
+        return size_t(16) << 30;
+    }();
+    return limit;
+}
+
+// Frees every cached block of `device` (all devices for device < 0); returns the bytes freed.
+size_t release_cached_blocks(int device) {
+    BlockCache& c = block_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    size_t freed = 0;
+    int cur = 0;
+    const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
+    for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
+        if (device >= 0 && it->first.first != device) { ++it; continue; }
+        cudaSetDevice(it->first.first);
+        for (void* p : it->second) {
+            cudaFree(p);
+            freed += it->first.second;
+        }
+        c.cached_bytes -= it->first.second * it->second.size();
+        it = c.free_blocks.erase(it);
+    }
+    if (have_cur) cudaSetDevice(cur);
+    return freed;
+}
 
 cudaError_t cached_alloc(void** p, size_t bytes, int* device) {
     int dev = 0;
@@ -227,7 +261,7 @@ const char* vajra_status_string(vajra_status s) {
         case VAJRA_ERR_NO_DEVICE: return "no CUDA device";
         case VAJRA_ERR_CUDA: return "CUDA error";
         case VAJRA_ERR_OUT_OF_MEMORY: return "out of device memory";
-        case VAJRA_ERR_WAIT_TIMEOUT: return "device wait timed out";
+        case VAJRA_ERR_WAIT_TIMEOUT: return "device wait timed out (reserved)";
         case VAJRA_ERR_INTERNAL: return "internal error";
         default: return "unknown status";
     }
@@ -470,6 +504,50 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
     return s;
 }
 
+vajra_status vajra_scale_lp(const vajra_lp* lp, const vajra_opts* opts, double* row_scale, double* col_scale,
+                            double* values, double* c, double* col_lower, double* col_upper, double* row_lower,
+                            double* row_upper) {
+    vajra_opts o;
+    if (opts) o = *opts; else vajra_default_opts(&o);
+    o.algorithm = VAJRA_ALGO_HALPERN;
+    vajra_pdhg* h = nullptr;
+    vajra_status s = vajra_pdhg_create(lp, &o, &h);
+    if (s != VAJRA_OK) return s;
+    struct Guard { vajra_pdhg* h; ~Guard() { vajra_pdhg_destroy(h); } } guard{h};
+    const int m = h->m, n = h->n;
+    if (m == 0 || n == 0) { set_error("vajra_scale_lp: an LP without rows or columns is not scaled"); return VAJRA_ERR_INVALID_ARGUMENT; }
+    cudaStream_t st = h->stream;
+    Prepared p;
+    DeviceBuffer<SetupState> sst;
+    VJ_TRY(sst.alloc(1));
+    VJ_TRY(build_csr(h->lp, p, st));
+    ScalingOpts so;
+    so.enable = o.enable_scaling != 0;
+    so.ruiz_iterations = o.ruiz_iterations > 0 ? o.ruiz_iterations : 10;
+    so.ruiz_tolerance = 0.05;
+    so.pock_chambolle = o.pock_chambolle != 0;
+    so.negate_c = h->sense != 0;
+    VJ_TRY(prepare_scaled(h->lp, p, so, sst.get(), st));
+    auto out = [&](double* dst, const DeviceBuffer<double>& src, int64_t k) -> vajra_status {
+        if (dst && k > 0) VJ_CUDA(cudaMemcpyAsync(dst, src.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, st));
+        return VAJRA_OK;
+    };
+    VJ_TRY(out(row_scale, p.row_scale, m));
+    VJ_TRY(out(col_scale, p.col_scale, n));
+    VJ_TRY(out(values, p.csc_val, h->nnz));
+    VJ_TRY(out(c, p.c, n));
+    VJ_TRY(out(col_lower, p.col_lower, n));
+    VJ_TRY(out(col_upper, p.col_upper, n));
+    VJ_TRY(out(row_lower, p.row_lower, m));
+    VJ_TRY(out(row_upper, p.row_upper, m));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    return VAJRA_OK;
+}
+
+int64_t vajra_release_cached_memory(int32_t device) {
+    return static_cast<int64_t>(release_cached_blocks(device));
+}
+
 void vajra_default_unrolled_opts(vajra_unrolled_opts* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
@@ -611,18 +689,23 @@ struct EpiStepPrimal {
     }
 };
 
-// compute_diagnostics_device_kernel semantics (spmv_kernels.cuh:210-278) with a
-// deterministic single-CTA reduction.
-__global__ void __launch_bounds__(1024)
-k_device_diagnostics(int m, int n, const double* __restrict__ ax, const double* __restrict__ rl,
-                     const double* __restrict__ ru, const double* __restrict__ aty, const double* __restrict__ c,
-                     const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ cl,
-                     const double* __restrict__ cu, vajra_device_diagnostics* out) {
+// compute_diagnostics_device_kernel semantics (spmv_kernels.cuh:210-278) over a grid of CTAs
+// with a deterministic two-stage reduction: each CTA writes its maxima (primal, dual, NaN flag)
+// and its objective partial in a fixed order, then one CTA combines the partials in CTA order.
+constexpr int kDiagQ = 4;
+constexpr int kDiagMaxBlocks = 148 * 4;
+
+__global__ void __launch_bounds__(kThreads)
+k_diag_part(int m, int n, const double* __restrict__ ax, const double* __restrict__ rl, const double* __restrict__ ru,
+            const double* __restrict__ aty, const double* __restrict__ c, const double* __restrict__ x,
+            const double* __restrict__ y, const double* __restrict__ cl, const double* __restrict__ cu,
+            double* __restrict__ part) {
     __shared__ double red_max[3 * 32];
     __shared__ double red_sum[32];
     double mx[3] = {0.0, 0.0, 0.0};   // primal, dual, nan flag
     double sm[1] = {0.0};
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
         const double a = ax[i], yi = y[i];
         if (isnan(a) || isinf(a) || isnan(yi) || isinf(yi)) mx[2] = 1.0;
         double viol = 0.0;
@@ -630,7 +713,7 @@ k_device_diagnostics(int m, int n, const double* __restrict__ ax, const double* 
         if (a > ru[i]) viol = a - ru[i];
         if (viol > mx[0]) mx[0] = viol;
     }
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
         const double xj = x[j], cj = c[j], atyj = aty[j];
         if (isnan(xj) || isinf(xj) || isnan(cj) || isinf(cj) || isnan(atyj) || isinf(atyj)) mx[2] = 1.0;
         const double lj = cl[j], uj = cu[j];
@@ -645,6 +728,25 @@ k_device_diagnostics(int m, int n, const double* __restrict__ ax, const double* 
         if (lj <= -1e20 && uj >= 1e20) d = fabs(dj);
         if (d > mx[1]) mx[1] = d;
         sm[0] += cj * xj;
+    }
+    block_reduce<OpMax, double, 3>(mx, red_max);
+    block_reduce<OpSum, double, 1>(sm, red_sum);
+    if (threadIdx.x == 0) {
+        double* q = part + static_cast<size_t>(blockIdx.x) * kDiagQ;
+        q[0] = mx[0]; q[1] = mx[1]; q[2] = mx[2]; q[3] = sm[0];
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+k_diag_final(int nb, const double* __restrict__ part, vajra_device_diagnostics* out) {
+    __shared__ double red_max[3 * 32];
+    __shared__ double red_sum[32];
+    double mx[3] = {0.0, 0.0, 0.0};
+    double sm[1] = {0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        const double* q = part + static_cast<size_t>(b) * kDiagQ;
+        for (int k = 0; k < 3; ++k) mx[k] = q[k] > mx[k] ? q[k] : mx[k];
+        sm[0] += q[3];
     }
     block_reduce<OpMax, double, 3>(mx, red_max);
     block_reduce<OpSum, double, 1>(sm, red_sum);
@@ -722,9 +824,20 @@ vajra_status vajra_device_diagnostics_f64(int32_t rows, int32_t cols, const doub
                                           const double* x, const double* y, const double* col_lower,
                                           const double* col_upper, vajra_device_diagnostics* out, void* stream) {
     if (rows < 0 || cols < 0 || !out) return VAJRA_ERR_INVALID_ARGUMENT;
-    k_device_diagnostics<<<1, 1024, 0, VJ_STREAM(stream)>>>(rows, cols, ax, row_lower, row_upper, aty, c, x, y,
-                                                           col_lower, col_upper, out);
-    VJ_LAUNCH_CHECK();
+    cudaStream_t st = VJ_STREAM(stream);
+    const int64_t work = rows > cols ? rows : cols;
+    const int nb = static_cast<int>(grid_for(work > 0 ? work : 1, kThreads, kDiagMaxBlocks));
+    // The block partials come from the stream-ordered pool on the caller's stream (no device
+    // synchronisation, and usable inside a stream capture).
+    double* part = nullptr;
+    VJ_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&part), sizeof(double) * kDiagQ * nb, st));
+    k_diag_part<<<nb, kThreads, 0, st>>>(rows, cols, ax, row_lower, row_upper, aty, c, x, y, col_lower, col_upper,
+                                          part);
+    k_diag_final<<<1, 1024, 0, st>>>(nb, part, out);
+    const cudaError_t le = cudaGetLastError();
+    VJ_CUDA(cudaFreeAsync(part, st));
+    VJ_CUDA(le);
+    note_launch(2);
     return VAJRA_OK;
 }
 

@@ -58,6 +58,7 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
 cudaError_t cached_alloc(void** p, size_t bytes, int* device);
 void cached_release(void* p, size_t bytes, int device);
 size_t block_cache_limit();
+size_t release_cached_blocks(int device);
 
 // Owning device allocation.  Moves only; releases on destruction.
 template <typename T>

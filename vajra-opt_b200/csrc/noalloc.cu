@@ -10,9 +10,14 @@
 //
 // The per-block partial sums go to a file-scope device array of fixed size (2 MiB, loaded
 // with the library and held by every device that uses it until the process exits), which
-// limits an LP to 8,388,608 rows and columns here; larger sizes are rejected.  Host code cannot use the array's name as a device address,
-// so the first call on each device obtains that device's address with cudaGetSymbolAddress
-// (with the device current) and keeps it; make that first call before any stream capture.
+// limits an LP to 8,388,608 rows and columns here; larger sizes are rejected.  Host code
+// cannot use the array's name as a device address, so each call looks up the current
+// device's address with cudaGetSymbolAddress (with that device current) whenever its stream
+// is not being captured, and keeps it per device.  A call made during a stream capture uses
+// the address kept by the last call outside a capture on that device, so make the first call
+// on a device before any capture -- and, after a cudaDeviceReset or a reset of the primary
+// context (which reloads the library's module, so the array may move), make one call outside
+// a capture before capturing again.
 // Every call on a device shares the one array and overwrites it: calls that overlap on the
 // GPU (different streams, or host threads without ordering) race and give wrong results.
 // Each call writes every partial it later reads, so nothing needs clearing between calls.
@@ -125,17 +130,27 @@ k_na_final(int nb_r, int nb_c, const double* __restrict__ part_r, const double* 
     out[5] = dobj;
 }
 
-// The current device's address of g_noalloc_scratch (obtained once per device).
-vajra_status scratch_address(double** out) {
+// The current device's address of g_noalloc_scratch.  Looked up afresh on every call whose
+// stream is not capturing (a reset context reloads the module, and the array can move); a
+// call inside a capture cannot make that lookup and uses the address the last such call kept.
+vajra_status scratch_address(cudaStream_t st, double** out) {
     int dev = 0;
     VJ_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) { set_error("device ordinal %d beyond %d", dev, kMaxDevices); return VAJRA_ERR_INVALID_ARGUMENT; }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    const cudaError_t ce = cudaStreamIsCapturing(st, &cap);
+    const bool capturing = ce != cudaSuccess || cap != cudaStreamCaptureStatusNone;
+    if (ce != cudaSuccess) cudaGetLastError();   // e.g. the legacy stream while another captures
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
+    if (!capturing) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
         g_scratch_addr[dev] = static_cast<double*>(p);
+    } else if (!g_scratch_addr[dev]) {
+        set_error("vajra_relative_kkt_noalloc_f64: first call on device %d made inside a stream capture; "
+                  "make one call outside a capture first", dev);
+        return VAJRA_ERR_INVALID_ARGUMENT;
     }
     *out = g_scratch_addr[dev];
     return VAJRA_OK;
@@ -151,9 +166,12 @@ extern "C" vajra_status vajra_relative_kkt_noalloc_f64(
     const int64_t* col_ptr, const int32_t* row_idx, const double* csc_values, const double* c,
     const double* col_lower, const double* col_upper, const double* row_lower, const double* row_upper,
     const double* x, const double* y, int32_t sense, double objective_offset, double* out, void* stream) {
-    if (rows < 1 || cols < 1 || !row_ptr || !col_idx || !csr_values || !col_ptr || !row_idx || !csc_values || !c ||
-        !col_lower || !col_upper || !row_lower || !row_upper || !x || !y || !out) {
-        set_error("vajra_relative_kkt_noalloc_f64: empty LP or NULL pointer");
+    // An LP without rows (column bounds only) is allowed: its row-side arrays may be NULL.
+    const bool has_rows = rows > 0;
+    if (rows < 0 || cols < 1 || !col_ptr || !c || !col_lower || !col_upper || !x || !out ||
+        (has_rows && (!row_ptr || !col_idx || !csr_values || !row_idx || !csc_values || !row_lower || !row_upper ||
+                      !y))) {
+        set_error("vajra_relative_kkt_noalloc_f64: negative row count, no columns, or a NULL pointer");
         return VAJRA_ERR_INVALID_ARGUMENT;
     }
     if (rows > kNaMaxExtent || cols > kNaMaxExtent) {
@@ -162,18 +180,19 @@ extern "C" vajra_status vajra_relative_kkt_noalloc_f64(
                   rows, cols, static_cast<long long>(kNaMaxExtent));
         return VAJRA_ERR_INVALID_ARGUMENT;
     }
-    double* scratch = nullptr;
-    VJ_TRY(scratch_address(&scratch));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* scratch = nullptr;
+    VJ_TRY(scratch_address(st, &scratch));
     const int nb_r = (rows + kNaRowsPerBlock - 1) / kNaRowsPerBlock;
     const int nb_c = (cols + kNaRowsPerBlock - 1) / kNaRowsPerBlock;
     double* part_r = scratch;
     double* part_c = scratch + static_cast<size_t>(kNaMaxBlocks) * kNaQ;
-    k_na_rows<<<nb_r, kThreads, 0, st>>>(rows, row_ptr, col_idx, csr_values, x, y, row_lower, row_upper, part_r);
+    if (has_rows)
+        k_na_rows<<<nb_r, kThreads, 0, st>>>(rows, row_ptr, col_idx, csr_values, x, y, row_lower, row_upper, part_r);
     k_na_cols<<<nb_c, kThreads, 0, st>>>(cols, col_ptr, row_idx, csc_values, x, y, c, col_lower, col_upper, sense,
                                          part_c);
     k_na_final<<<1, 1024, 0, st>>>(nb_r, nb_c, part_r, part_c, sense ? -objective_offset : objective_offset, out);
-    note_launch(3);
+    note_launch(has_rows ? 3 : 2);
     VJ_LAUNCH_CHECK();
     return VAJRA_OK;
 }

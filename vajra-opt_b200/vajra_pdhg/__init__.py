@@ -21,7 +21,7 @@ STATUS_NAMES = {0: "NOT_SOLVED", 1: "OPTIMAL", 2: "INFEASIBLE", 3: "UNBOUNDED",
                 11: "UNSUPPORTED"}
 
 __all__ = ["solve", "solve_batch", "Solver", "default_opts", "probe_device", "is_cuda_available",
-           "last_timing", "ALGO_REFERENCE", "ALGO_HALPERN", "PREC_FP64", "PREC_MIXED",
+           "last_timing", "scale_lp", "release_cached_memory", "ALGO_REFERENCE", "ALGO_HALPERN", "PREC_FP64", "PREC_MIXED",
            "STATUS_NAMES"]
 
 
@@ -165,3 +165,24 @@ def last_timing() -> dict:
     d["device_name"] = d["device_name"].decode(errors="replace")
     d["kernel_mode"] = d["kernel_mode"].decode(errors="replace")
     return d
+
+
+def scale_lp(lp, **opts) -> dict:
+    """The device set-up's scaling of `lp` (vajra_scale_lp): Ruiz, then Pock-Chambolle when
+    `pock_chambolle` is on.  Returns the cumulative row / column scales, the scaled values in
+    CSC order, the scaled c (negated for maximisation) and the scaled bounds."""
+    h = _HostLp(lp)
+    o = default_opts(**opts)
+    m, n = int(lp.num_rows), int(lp.num_cols)
+    out = {"row_scale": np.zeros(m), "col_scale": np.zeros(n), "values": np.zeros(int(h.col_ptr[-1])),
+           "c": np.zeros(n), "col_lower": np.zeros(n), "col_upper": np.zeros(n), "row_lower": np.zeros(m),
+           "row_upper": np.zeros(m)}
+    keys = ("row_scale", "col_scale", "values", "c", "col_lower", "col_upper", "row_lower", "row_upper")
+    st = _capi.lib().vajra_scale_lp(C.byref(h.s), C.byref(o), *[C.c_void_p(out[k].ctypes.data) for k in keys])
+    _capi.check(st, "vajra_scale_lp")
+    return out
+
+
+def release_cached_memory(device: int = -1) -> int:
+    """Return the library's cached device blocks to the driver (vajra_release_cached_memory)."""
+    return int(_capi.lib().vajra_release_cached_memory(device))

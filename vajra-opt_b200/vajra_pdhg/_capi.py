@@ -112,6 +112,8 @@ SIGNATURES = [
     ("vajra_pdhg_step_f64", C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 11 + [C.c_double, C.c_double] + [C.c_void_p] * 6),
     ("vajra_relative_kkt_noalloc_f64", C.c_int32, [C.c_int32, C.c_int32] + [C.c_void_p] * 13
      + [C.c_int32, C.c_double, C.c_void_p, C.c_void_p]),
+    ("vajra_scale_lp", C.c_int32, [C.POINTER(VajraLp), C.POINTER(VajraOpts)] + [C.c_void_p] * 8),
+    ("vajra_release_cached_memory", C.c_int64, [C.c_int32]),
 ]
 
 _lib = None
