@@ -62,6 +62,10 @@ def parse():
                          "profiler would distort")
     ap.add_argument("--degree-order", type=int, default=0, choices=[-1, 0, 1],
                     help="row / column renumbering by entry count: 0 auto (on from 2^20 entries), 1 on, -1 off")
+    ap.add_argument("--pow2-scaling", type=int, default=None, choices=[0, 1],
+                    help="round the scale factors to powers of two (library default when omitted)")
+    ap.add_argument("--fp64-value-storage", type=int, default=None, choices=[0, 1, 2],
+                    help="FP64 iterations on the exact FP32 copy of the values: 0 auto, 1 never, 2 also the FP64 form")
     ap.add_argument("--batch", type=int, default=0,
                     help="batched workload instead: this many config-0-style LPs (m log-uniform on "
                          "[100, 20000]), one batched solve vs the same LPs solved one after another")
@@ -502,13 +506,18 @@ def run(args, world, rank, local, dist):
         if args.shapes:
             sa, sat = (int(v) for v in args.shapes.split(","))
             shapes = dict(spmv_shape_a=sa, spmv_shape_at=sat, autotune=0)
+        knobs = {k: v for k, v in (("pow2_scaling", args.pow2_scaling),
+                                   ("fp64_value_storage", args.fp64_value_storage)) if v is not None}
         r = V.solve(lp, precision=prec, iteration_limit=args.profile_iters, device=local,
-                    mixed_switch_tolerance=0.0, mixed_stall_checks=0, degree_order=args.degree_order, **shapes)
+                    mixed_switch_tolerance=0.0, mixed_stall_checks=0, degree_order=args.degree_order, **shapes,
+                    **knobs)
         print(json.dumps({"profile_iters": r["iterations"], "status": r["status_name"], "rel_kkt": r["rel_kkt"],
                           "groups": [r["spmv_group_a"], r["spmv_group_at"]],
                           "primal_us": r["primal_kernel_us"], "dual_us": r["dual_kernel_us"],
                           "primal_bytes": r["primal_kernel_bytes"], "dual_bytes": r["dual_kernel_bytes"]}))
         return 0
+    knobs = {k: v for k, v in (("pow2_scaling", args.pow2_scaling), ("fp64_value_storage", args.fp64_value_storage))
+             if v is not None}
     plp = pinned_copy(lp)
     # The first end-to-end call of a fresh process: it pays the SpMV autotuning (~0.4 s on this
     # LP) and the first device allocations, which every later call finds cached.
@@ -516,7 +525,7 @@ def run(args, world, rank, local, dist):
     if not args.no_e2e:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rc0 = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
+        rc0 = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order, **knobs)
         cold = {"wall_s": round(time.perf_counter() - t0, 4), "setup_s": round(rc0["setup_time_sec"], 4),
                 "status": rc0["status_name"]}
 
@@ -533,7 +542,7 @@ def run(args, world, rank, local, dist):
         return float(t.item())
 
     # ---- mixed precision, resident LP ----------------------------------------------
-    solver = V.Solver(lp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
+    solver = V.Solver(lp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order, **knobs)
     for _ in range(args.warmup):
         solver.run()
     barrier()
@@ -563,7 +572,7 @@ def run(args, world, rank, local, dist):
     # ---- plain FP64 form --------------------------------------------------------------
     fp64 = None
     if args.fp64_steps > 0:
-        s64 = V.Solver(lp, precision=V.PREC_FP64, device=local, degree_order=args.degree_order)
+        s64 = V.Solver(lp, precision=V.PREC_FP64, device=local, degree_order=args.degree_order, **knobs)
         s64.run()
         r64 = [s64.run() for _ in range(args.fp64_steps)]
         s64.close()
@@ -579,7 +588,7 @@ def run(args, world, rank, local, dist):
         e2e_times = []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            r = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order)
+            r = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order, **knobs)
             e2e_times.append(time.perf_counter() - t0)
         barrier()
         h2d = 8 * (lp.num_cols + 1) + 12 * lp.nnz + 8 * (3 * lp.num_cols + 2 * lp.num_rows)

@@ -29,7 +29,7 @@ extern "C" {
 
 /* Layout version of the structs below.  A caller compiled against one version must not call
  * a library of another: compare with vajra_abi_version() before the first call. */
-#define VAJRA_ABI_VERSION 7
+#define VAJRA_ABI_VERSION 8
 
 typedef int32_t vajra_status;
 enum {
@@ -71,9 +71,10 @@ enum {
 /* Precision of VAJRA_ALGO_HALPERN (VAJRA_ALGO_REFERENCE is always FP64). */
 enum {
     VAJRA_PREC_FP64 = 0,   /* "plain" form: FP64 values, iterates and accumulation       */
-    VAJRA_PREC_MIXED = 1   /* FP32 values/iterates/SpMV accumulation, FP64 KKT, gap,
+    VAJRA_PREC_MIXED = 1,  /* FP32 values/iterates/SpMV accumulation, FP64 KKT, gap,
                               restart and primal-weight decisions, then an FP64 polish
                               restarted from the FP32 iterate                            */
+    VAJRA_PREC_FP32 = 2    /* vajra_pdhg_unrolled only: the FP32 map and reverse pass    */
 };
 
 /* The reference Model (include/indus/model.hpp:16-55) as CSC host arrays. */
@@ -140,6 +141,15 @@ typedef struct vajra_opts {
                                    gather most often share cache lines; results come back in
                                    the caller's numbering.  0 auto (on from 2^20 entries),
                                    1 on, -1 off                                            */
+    int32_t pow2_scaling;       /* HALPERN: 1 = round the final row / column scale factors to
+                                   the nearest power of two, so that scaling is exact: a
+                                   matrix whose values fit FP32 still fits it once scaled (0) */
+    int32_t fp64_value_storage; /* HALPERN FP64 iterations and every FP64 check: where each
+                                   scaled value is exactly an FP32 number, read the FP32 copy
+                                   of the matrix (4 bytes an entry instead of 8; FP64 vectors
+                                   and sums, so every result is bit-identical).  0 auto (MIXED:
+                                   on when exact; FP64 form: off), 1 FP64 copy always, 2 the
+                                   FP32 copy when exact in either precision                  */
     int32_t reserved;
 } vajra_opts;
 
@@ -284,7 +294,11 @@ typedef struct vajra_unrolled_opts {
     int32_t iterations;         /* unrolled iterations K (2000)                          */
     int32_t checkpoint_every;   /* forward checkpoint interval (100); segments between
                                    checkpoints are recomputed in the reverse pass         */
-    int32_t precision;          /* VAJRA_PREC_MIXED: FP32 map; VAJRA_PREC_FP64: FP64 map  */
+    int32_t precision;          /* VAJRA_PREC_MIXED (default): the FP64 map -- forward pass,
+                                   checkpoints and the active sets recomputed per segment --
+                                   with the reverse pass (cotangents, transposed SpMVs) in
+                                   FP32; VAJRA_PREC_FP64: FP64 throughout; VAJRA_PREC_FP32:
+                                   the FP32 map and reverse pass                          */
     int32_t enable_scaling;     /* Ruiz + Pock-Chambolle (constants of A)                */
     double step_safety;         /* 0.95                                                   */
     int32_t device;

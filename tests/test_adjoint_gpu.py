@@ -1,12 +1,12 @@
-"""Adjoint of the unrolled PDHG map (vajra_pdhg_unrolled) against FP64 one-sided finite
-differences of the same map (kink-aware), checkpoint invariance, the torch.autograd harness,
-and the optimal-value gradient y* = dV/db from the reference's own dual simplex."""
+"""Adjoint of the unrolled PDHG map (vajra_pdhg_unrolled) against FP64 finite differences of
+the same map (kink-aware), checkpoint invariance, the torch.autograd harness, and the
+optimal-value gradient dV/db = y* against the reference's own dual simplex."""
 import numpy as np
 import pytest
 
 from oracle import bindings as B
 from vajra_pdhg import workloads as W
-from vajra_pdhg.autograd import PREC_FP64, PREC_MIXED, unrolled
+from vajra_pdhg.autograd import PREC_FP32, PREC_FP64, PREC_MIXED, unrolled
 
 pytestmark = pytest.mark.gpu
 
@@ -54,6 +54,9 @@ def fd_directional(lps, w, dc, db, h, **opts):
 
 @pytest.mark.parametrize("prec,tol", [(PREC_FP64, 1e-6), (PREC_MIXED, 1e-4)])
 def test_adjoint_matches_fp64_finite_differences(cuda, prec, tol):
+    """A direction whose forward and backward differences agree (no active-set change within
+    +-h) must match the adjoint to `tol`; only a direction flagged by a disagreement may miss,
+    and then the adjoint must still match one side (a change on one side only)."""
     lps = batch()
     rng = np.random.default_rng(1)
     N = sum(lp.num_cols for lp in lps)
@@ -62,16 +65,40 @@ def test_adjoint_matches_fp64_finite_differences(cuda, prec, tol):
     opts = dict(iterations=300, checkpoint_every=50)
     g = unrolled(lps, w, precision=prec, **opts)
     gb = g["grad_row_lower"] + g["grad_row_upper"]
-    errs, misses = [], []
-    while len(errs) < 8:
-        # a wrong adjoint misses in every direction; a kink on both sides of 0 is rare
-        assert len(misses) <= 4, (errs, misses)
+    clean, flagged = [], 0
+    for _ in range(16):
         dc = rng.standard_normal(N)
         db = rng.standard_normal(M)
         adj = g["grad_c"] @ dc + gb @ db
-        e = min(abs(adj - fd) / max(1e-12, abs(fd)) for fd in fd_directional(lps, w, dc, db, 1e-7, **opts))
-        (errs if e <= tol else misses).append(e)
-    assert max(errs) <= tol, errs
+        fwd, bwd = fd_directional(lps, w, dc, db, 1e-7, **opts)
+        rel = [abs(adj - fd) / max(1e-12, abs(fd)) for fd in (fwd, bwd)]
+        if abs(fwd - bwd) <= 1e-7 * max(abs(fwd), abs(bwd)):
+            clean.append(max(rel))
+        else:
+            flagged += 1
+            assert min(rel) <= tol, (rel, fwd, bwd, adj)
+    assert len(clean) >= 8, (clean, flagged)
+    assert max(clean) <= tol, clean
+
+
+def test_fp32_map_adjoint_against_its_own_active_sets(cuda):
+    """The pure FP32 map (PREC_FP32): its derivative differs from the FP64 map's only where an
+    active set flipped; on this short map it still matches FP64 differences to 1e-3."""
+    lps = batch()
+    rng = np.random.default_rng(5)
+    N = sum(lp.num_cols for lp in lps)
+    M = sum(lp.num_rows for lp in lps)
+    w = rng.standard_normal(N)
+    opts = dict(iterations=300, checkpoint_every=50)
+    g = unrolled(lps, w, precision=PREC_FP32, **opts)
+    gb = g["grad_row_lower"] + g["grad_row_upper"]
+    errs = []
+    for _ in range(8):
+        dc = rng.standard_normal(N)
+        db = rng.standard_normal(M)
+        adj = g["grad_c"] @ dc + gb @ db
+        errs.append(min(abs(adj - fd) / max(1e-12, abs(fd)) for fd in fd_directional(lps, w, dc, db, 1e-7, **opts)))
+    assert np.median(errs) <= 1e-3, errs
 
 
 def test_checkpoint_interval_does_not_change_gradients(cuda):
@@ -103,15 +130,30 @@ def test_autograd_function(cuda):
 
 
 @pytest.mark.skipif(not B.ref_available(), reason="needs the reference's dual simplex (oracle/_ref)")
-def test_objective_gradient_wrt_b_approaches_simplex_duals(cuda):
-    """dV/db = y* (unique here); the unrolled map's derivative of c.x(K) approaches it as K
-    grows (slowly: the plain unrolled iteration has no restarts)."""
-    lp = W.random_planted(60, 150, 5, seed=44)
+@pytest.mark.parametrize("m,n,seed", [(60, 150, 44), (200, 500, 45)])
+def test_optimal_value_gradient_matches_simplex_duals(cuda, m, n, seed):
+    """dV/db of V(c, b) = min c.x (the OptimalValue harness: the restarted Halpern solver to
+    FP64 relative KKT 1e-10, envelope-theorem backward) against the reference dual simplex's
+    y* (src/engine/model.cpp:528-614) to 1e-4, and against central differences of V itself."""
+    import torch
+    from vajra_pdhg.autograd import OptimalValue
+    lp = W.random_planted(m, n, 5, seed=seed)
     s = B.ref_solve(lp, algorithm="dual_simplex", through_solve=True, iteration_limit=100000)
     assert s["status_name"] == "OPTIMAL"
-    rel = {}
-    for k in (5000, 20000):
-        g = unrolled([lp], None, iterations=k, checkpoint_every=500, precision=PREC_FP64)
-        gb = g["grad_row_lower"] + g["grad_row_upper"]
-        rel[k] = np.linalg.norm(gb - s["y"]) / np.linalg.norm(s["y"])
-    assert rel[20000] < rel[5000] and rel[20000] <= 0.05, rel
+    c = torch.tensor(lp.c, dtype=torch.float64, requires_grad=True)
+    b = torch.tensor(lp.row_lower, dtype=torch.float64, requires_grad=True)
+    v = OptimalValue.apply(c, b, [lp], None)
+    v.sum().backward()
+    y = b.grad.numpy()
+    assert abs(v.item() - s["objective_value"]) <= 1e-8 * (1 + abs(s["objective_value"]))
+    assert np.linalg.norm(y - s["y"]) <= 1e-4 * np.linalg.norm(s["y"]), np.linalg.norm(y - s["y"])
+    # V is piecewise linear in b: central differences along a few directions
+    rng = np.random.default_rng(seed)
+    h = 1e-5 * np.linalg.norm(lp.row_lower)
+    for _ in range(3):
+        d = rng.standard_normal(m)
+        d /= np.linalg.norm(d)
+        vp = OptimalValue.apply(c.detach(), b.detach() + h * torch.from_numpy(d), [lp], None).item()
+        vm = OptimalValue.apply(c.detach(), b.detach() - h * torch.from_numpy(d), [lp], None).item()
+        fd = (vp - vm) / (2 * h)
+        assert abs(fd - y @ d) <= 1e-4 * np.linalg.norm(y), (fd, y @ d)

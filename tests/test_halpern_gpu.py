@@ -291,3 +291,65 @@ def test_sliced_ell_shape_without_ordering(cuda):
     g = V.solve(lp, precision=V.PREC_FP64, degree_order=-1, spmv_shape_a=-3, spmv_shape_at=-3)
     assert g["spmv_group_a"] == 128 and g["spmv_group_at"] == 128
     check_solution(lp, g, obj=highs(lp))
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_sliced_ell_hot_prefix_shape_reaches_the_optimum(cuda, prec):
+    """The sliced-ELL kernels that serve the first vector entries from shared memory (shape
+    -4, reported as 129), forced for both SpMVs."""
+    lp = W.random_planted(600, 1500, (2, 40), seed=31)
+    g = V.solve(lp, precision=prec, degree_order=1, spmv_shape_a=-4, spmv_shape_at=-4)
+    assert g["spmv_group_a"] == 129 and g["spmv_group_at"] == 129
+    check_solution(lp, g, obj=lp.planted_objective)
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_sliced_ell_hot_prefix_is_bit_identical_to_sliced_ell(cuda, prec):
+    """Same row sums in the same order, only the source of the gathered entries differs: 64
+    iterations with shape -4 and with shape -3 give the same bits.  The LP has a row above 4096
+    entries (one CTA), columns of 128..4096 entries (one warp) and more columns than the hot
+    prefix holds in FP64 (14,336) and in FP32 (28,672)."""
+    base = W.small_random(2600, 40000, 12)
+    lp = with_structure(base, dense_row=7, dense_col=11, empty_rows=(3, 50), empty_cols=(0, 99), seed=1)
+    kw = dict(precision=prec, iteration_limit=64, degree_order=1)
+    a = V.solve(lp, spmv_shape_a=-4, spmv_shape_at=-4, **kw)
+    b = V.solve(lp, spmv_shape_a=-3, spmv_shape_at=-3, **kw)
+    assert a["spmv_group_a"] == 129 and b["spmv_group_a"] == 128
+    for k in ("x", "y", "d", "row_value"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def fp32_exact(lp):
+    """lp with its matrix values rounded to FP32 (every value then fits FP32 exactly)."""
+    out = W.LP(**{**lp.__dict__})
+    out.values = np.asarray(lp.values, np.float32).astype(np.float64)
+    return out
+
+
+@pytest.mark.parametrize("prec", PRECISIONS)
+def test_power_of_two_scaling_reaches_the_optimum(cuda, prec):
+    lp = W.small_random(300, 700, 3)
+    g = V.solve(lp, precision=prec, pow2_scaling=1)
+    check_solution(lp, g, obj=highs(lp))
+
+
+@pytest.mark.parametrize("shape", [-1, -3, -4])
+def test_fp64_iterations_on_the_exact_fp32_copy_are_bit_identical(cuda, shape):
+    """With power-of-two scaling an LP whose values fit FP32 keeps fitting FP32 once scaled; the
+    FP64 iterations and checks may then read the FP32 copy of the matrix (FP64 vectors and
+    sums): 256 iterations give the same bits as with the FP64 copy."""
+    lp = fp32_exact(W.random_planted(900, 4000, (2, 50), seed=34))
+    kw = dict(precision=V.PREC_FP64, iteration_limit=256, degree_order=1, pow2_scaling=1, spmv_shape_a=shape,
+              spmv_shape_at=shape)
+    a = V.solve(lp, fp64_value_storage=2, **kw)
+    b = V.solve(lp, fp64_value_storage=1, **kw)
+    assert a["primal_kernel_bytes"] < b["primal_kernel_bytes"]      # the 4-byte copy was read
+    for k in ("x", "y", "d", "row_value"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert a["rel_kkt"] == b["rel_kkt"]
+
+
+def test_mixed_polish_on_the_exact_fp32_copy_reaches_the_optimum(cuda):
+    lp = fp32_exact(W.random_planted(2000, 5000, 8, seed=1))
+    g = V.solve(lp, precision=V.PREC_MIXED, pow2_scaling=1, degree_order=1)
+    check_solution(lp, g, obj=lp.planted_objective)

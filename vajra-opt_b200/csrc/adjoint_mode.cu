@@ -164,34 +164,50 @@ __global__ void k_steps(int count, const double* __restrict__ sigma_max, double 
     if (i < count) step[i] = safety / (sigma_max[i] > 1e-12 ? sigma_max[i] : 1.0);
 }
 
-template <typename T>
+// TF: type of the forward map (values, iterates, checkpoints, masks come from it); TB: type
+// of the reverse pass (cotangents and the transposed SpMVs).
+template <typename TF, typename TB>
 struct Unrolled {
     int m = 0, n = 0;
     CsrView a, at;
-    const T* csr_val = nullptr;
-    const T* csc_val = nullptr;
-    DeviceBuffer<T> c, cl, cu, rl, ru, x, xb, y, xh, yh, wh, preh, ckpt;
+    const TF* csr_val = nullptr;
+    const TF* csc_val = nullptr;
+    const TB* csr_val_b = nullptr;
+    const TB* csc_val_b = nullptr;
+    DeviceBuffer<TF> c, cl, cu, rl, ru, x, xb, y, ckpt;
+    DeviceBuffer<TB> xh, yh, wh, preh;
     DeviceBuffer<uint8_t> pmask, dmask;
     const int* row_inst = nullptr;
     const int* col_inst = nullptr;
     const double* step = nullptr;
 
     void forward_step(uint8_t* pm, uint8_t* dm, cudaStream_t st) {
-        launch_spmv_t<T, T, T>(at, csc_val, y.get(),
-                               EpiFwdPrimal<T>{c.get(), cl.get(), cu.get(), x.get(), xb.get(), col_inst, step, pm}, st);
-        launch_spmv_t<T, T, T>(a, csr_val, xb.get(), EpiFwdDual<T>{rl.get(), ru.get(), y.get(), row_inst, step, dm}, st);
+        launch_spmv_t<TF, TF, TF>(at, csc_val, y.get(),
+                                  EpiFwdPrimal<TF>{c.get(), cl.get(), cu.get(), x.get(), xb.get(), col_inst, step, pm}, st);
+        launch_spmv_t<TF, TF, TF>(a, csr_val, xb.get(), EpiFwdDual<TF>{rl.get(), ru.get(), y.get(), row_inst, step, dm}, st);
     }
     void backward_step(const uint8_t* pm, const uint8_t* dm, double* g_c, double* g_rl, double* g_ru,
                        cudaStream_t st) {
-        k_bwd_rows<T><<<grid_for(m), kThreads, 0, st>>>(m, dm, row_inst, step, yh.get(), wh.get(), g_rl, g_ru);
+        k_bwd_rows<TB><<<grid_for(m), kThreads, 0, st>>>(m, dm, row_inst, step, yh.get(), wh.get(), g_rl, g_ru);
         note_launch(1);
-        launch_spmv_t<T, T, T>(at, csc_val, wh.get(),
-                               EpiBwdPrimal<T>{xh.get(), preh.get(), g_c, pm, col_inst, step}, st);
-        launch_spmv_t<T, T, T>(a, csr_val, preh.get(), EpiBwdDual<T>{yh.get(), row_inst, step}, st);
+        launch_spmv_t<TB, TB, TB>(at, csc_val_b, wh.get(),
+                                  EpiBwdPrimal<TB>{xh.get(), preh.get(), g_c, pm, col_inst, step}, st);
+        launch_spmv_t<TB, TB, TB>(a, csr_val_b, preh.get(), EpiBwdDual<TB>{yh.get(), row_inst, step}, st);
     }
 };
 
 template <typename T>
+void values_of(Prepared& p, const T** csr, const T** csc) {
+    if constexpr (sizeof(T) == 4) {
+        *csr = p.csr_val32.get();
+        *csc = p.csc_val32.get();
+    } else {
+        *csr = p.csr_val.get();
+        *csc = p.csc_val.get();
+    }
+}
+
+template <typename TF, typename TB>
 vajra_status run_unrolled_t(const PackedHost& P, const vajra_unrolled_opts& o, Prepared& p, const DeviceLp& lp,
                             const int* row_inst, const int* col_inst, const int64_t* d_coff, const double* step,
                             const DeviceBuffer<double>& d_w, const double* c_orig_dev, double* h_loss, double* h_x,
@@ -201,22 +217,19 @@ vajra_status run_unrolled_t(const PackedHost& P, const vajra_unrolled_opts& o, P
     const int C = o.checkpoint_every > 0 ? o.checkpoint_every : 100;
     const int nseg = (K + C - 1) / C;
     const bool want_grad = h_gc || h_grl || h_gru;
-    Unrolled<T> U;
+    Unrolled<TF, TB> U;
     U.m = m; U.n = n;
     U.a = p.a; U.at = p.at;
     U.row_inst = row_inst; U.col_inst = col_inst; U.step = step;
-    if (sizeof(T) == 4) {
-        VJ_TRY(make_f32_values(p, P.nnz, st));
-        U.csr_val = reinterpret_cast<const T*>(p.csr_val32.get());
-        U.csc_val = reinterpret_cast<const T*>(p.csc_val32.get());
-    } else {
-        U.csr_val = reinterpret_cast<const T*>(p.csr_val.get());
-        U.csc_val = reinterpret_cast<const T*>(p.csc_val.get());
-    }
-    for (auto* b : {&U.c, &U.cl, &U.cu, &U.x, &U.xb, &U.xh, &U.preh}) VJ_TRY(b->alloc(n));
-    for (auto* b : {&U.rl, &U.ru, &U.y, &U.yh, &U.wh}) VJ_TRY(b->alloc(m));
-    auto conv = [&](const double* s, T* d, int k) {
-        if (k > 0) { k_convert_to<T><<<grid_for(k, kThreads, 148 * 32), kThreads, 0, st>>>(k, s, d); note_launch(1); }
+    if (sizeof(TF) == 4 || sizeof(TB) == 4) VJ_TRY(make_f32_values(p, P.nnz, st));
+    values_of<TF>(p, &U.csr_val, &U.csc_val);
+    values_of<TB>(p, &U.csr_val_b, &U.csc_val_b);
+    for (auto* b : {&U.c, &U.cl, &U.cu, &U.x, &U.xb}) VJ_TRY(b->alloc(n));
+    for (auto* b : {&U.rl, &U.ru, &U.y}) VJ_TRY(b->alloc(m));
+    for (auto* b : {&U.xh, &U.preh}) VJ_TRY(b->alloc(n));
+    for (auto* b : {&U.yh, &U.wh}) VJ_TRY(b->alloc(m));
+    auto conv = [&](const double* s, TF* d, int k) {
+        if (k > 0) { k_convert_to<TF><<<grid_for(k, kThreads, 148 * 32), kThreads, 0, st>>>(k, s, d); note_launch(1); }
     };
     conv(p.c.get(), U.c.get(), n);
     conv(p.col_lower.get(), U.cl.get(), n);
@@ -224,8 +237,8 @@ vajra_status run_unrolled_t(const PackedHost& P, const vajra_unrolled_opts& o, P
     conv(p.row_lower.get(), U.rl.get(), m);
     conv(p.row_upper.get(), U.ru.get(), m);
     const int mx = m > n ? m : n;
-    k_adj_init<T><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), U.x.get(), U.xb.get(),
-                                                    U.y.get());
+    k_adj_init<TF><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_lower.get(), p.col_upper.get(), U.x.get(), U.xb.get(),
+                                                     U.y.get());
     note_launch(1);
     if (want_grad) {
         VJ_TRY(U.ckpt.alloc(static_cast<size_t>(nseg) * (static_cast<size_t>(n) + m)));
@@ -239,41 +252,41 @@ vajra_status run_unrolled_t(const PackedHost& P, const vajra_unrolled_opts& o, P
     for (int s = 0; s < nseg; ++s) {
         const int len = (s + 1) * C <= K ? C : K - s * C;
         if (want_grad) {
-            VJ_CUDA(cudaMemcpyAsync(ck_x(s), U.x.get(), sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
-            VJ_CUDA(cudaMemcpyAsync(ck_y(s), U.y.get(), sizeof(T) * m, cudaMemcpyDeviceToDevice, st));
+            VJ_CUDA(cudaMemcpyAsync(ck_x(s), U.x.get(), sizeof(TF) * n, cudaMemcpyDeviceToDevice, st));
+            VJ_CUDA(cudaMemcpyAsync(ck_y(s), U.y.get(), sizeof(TF) * m, cudaMemcpyDeviceToDevice, st));
         }
         for (int k = 0; k < len; ++k) U.forward_step(nullptr, nullptr, st);
     }
     DeviceBuffer<double> loss, x_out, g_c, g_rl, g_ru;
     VJ_TRY(loss.alloc(count));
     VJ_TRY(x_out.alloc(n));
-    k_adj_loss<T><<<count, kThreads, 0, st>>>(d_coff, U.x.get(), p.col_scale.get(), d_w.get(), c_orig_dev, x_out.get(),
-                                              loss.get());
+    k_adj_loss<TF><<<count, kThreads, 0, st>>>(d_coff, U.x.get(), p.col_scale.get(), d_w.get(), c_orig_dev, x_out.get(),
+                                               loss.get());
     note_launch(1);
     VJ_LAUNCH_CHECK();
     if (want_grad) {
         VJ_TRY(g_c.alloc(n));
         VJ_TRY(g_rl.alloc(m));
         VJ_TRY(g_ru.alloc(m));
-        DeviceBuffer<T> x_final;
+        DeviceBuffer<TF> x_final;
         VJ_TRY(x_final.alloc(n));
-        VJ_CUDA(cudaMemcpyAsync(x_final.get(), U.x.get(), sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
-        k_adj_seed<T><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_scale.get(), d_w.get(), c_orig_dev, U.xh.get(),
-                                                        U.yh.get(), g_c.get(), g_rl.get(), g_ru.get());
+        VJ_CUDA(cudaMemcpyAsync(x_final.get(), U.x.get(), sizeof(TF) * n, cudaMemcpyDeviceToDevice, st));
+        k_adj_seed<TB><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_scale.get(), d_w.get(), c_orig_dev, U.xh.get(),
+                                                         U.yh.get(), g_c.get(), g_rl.get(), g_ru.get());
         note_launch(1);
         for (int s = nseg - 1; s >= 0; --s) {
             const int len = (s + 1) * C <= K ? C : K - s * C;
-            VJ_CUDA(cudaMemcpyAsync(U.x.get(), ck_x(s), sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
-            VJ_CUDA(cudaMemcpyAsync(U.y.get(), ck_y(s), sizeof(T) * m, cudaMemcpyDeviceToDevice, st));
+            VJ_CUDA(cudaMemcpyAsync(U.x.get(), ck_x(s), sizeof(TF) * n, cudaMemcpyDeviceToDevice, st));
+            VJ_CUDA(cudaMemcpyAsync(U.y.get(), ck_y(s), sizeof(TF) * m, cudaMemcpyDeviceToDevice, st));
             for (int k = 0; k < len; ++k)
                 U.forward_step(U.pmask.get() + static_cast<size_t>(k) * n, U.dmask.get() + static_cast<size_t>(k) * m, st);
             for (int k = len - 1; k >= 0; --k)
                 U.backward_step(U.pmask.get() + static_cast<size_t>(k) * n, U.dmask.get() + static_cast<size_t>(k) * m,
                                 g_c.get(), g_rl.get(), g_ru.get(), st);
         }
-        k_adj_finish<T><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_scale.get(), p.row_scale.get(), x_final.get(),
-                                                          g_c.get(), g_rl.get(), g_ru.get(), lp.row_lower.get(),
-                                                          lp.row_upper.get());
+        k_adj_finish<TF><<<grid_for(mx), kThreads, 0, st>>>(m, n, p.col_scale.get(), p.row_scale.get(), x_final.get(),
+                                                           g_c.get(), g_rl.get(), g_ru.get(), lp.row_lower.get(),
+                                                           lp.row_upper.get());
         note_launch(1);
         VJ_LAUNCH_CHECK();
         if (h_gc) VJ_CUDA(cudaMemcpyAsync(h_gc, g_c.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
@@ -332,11 +345,16 @@ vajra_status run_unrolled(int count, const vajra_lp* lps, const vajra_unrolled_o
     // the weight pointer handed to the kernels is null when no weights were given
     DeviceBuffer<double> none;
     const DeviceBuffer<double>& w = weights ? d_w : none;
+    // FP64: FP64 map and reverse pass.  MIXED: the FP64 map (forward, checkpoints and the
+    // recomputed active sets), reverse pass in FP32.  FP32: the FP32 map and reverse pass.
     if (o.precision == VAJRA_PREC_FP64)
-        return run_unrolled_t<double>(P, o, p, lp, row_inst.get(), col_inst.get(), d_coff.get(), step.get(), w,
-                                      lp.c.get(), h_loss, h_x, h_gc, h_grl, h_gru, st);
-    return run_unrolled_t<float>(P, o, p, lp, row_inst.get(), col_inst.get(), d_coff.get(), step.get(), w,
-                                 lp.c.get(), h_loss, h_x, h_gc, h_grl, h_gru, st);
+        return run_unrolled_t<double, double>(P, o, p, lp, row_inst.get(), col_inst.get(), d_coff.get(), step.get(), w,
+                                              lp.c.get(), h_loss, h_x, h_gc, h_grl, h_gru, st);
+    if (o.precision == VAJRA_PREC_FP32)
+        return run_unrolled_t<float, float>(P, o, p, lp, row_inst.get(), col_inst.get(), d_coff.get(), step.get(), w,
+                                            lp.c.get(), h_loss, h_x, h_gc, h_grl, h_gru, st);
+    return run_unrolled_t<double, float>(P, o, p, lp, row_inst.get(), col_inst.get(), d_coff.get(), step.get(), w,
+                                         lp.c.get(), h_loss, h_x, h_gc, h_grl, h_gru, st);
 }
 
 }  // namespace vajra

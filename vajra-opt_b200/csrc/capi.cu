@@ -136,6 +136,20 @@ void cached_release(void* p, size_t bytes, int device) {
     if (cur != device) cudaSetDevice(cur);
 }
 
+int sm_count() {
+    static std::mutex mu;
+    static std::map<int, int> counts;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = counts.find(dev);
+    if (it != counts.end()) return it->second;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    counts.emplace(dev, sms);
+    return sms;
+}
+
 void copy_out_vector(double* dst, const double* dev, int count, cudaStream_t st) {
     if (dst && count > 0) cudaMemcpyAsync(dst, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, st);
 }

@@ -363,6 +363,13 @@ struct Phase {
     const T* csc_val = nullptr;
     const T* sell_val_a = nullptr;    // the same values in sliced-ELL order (degree-ordered LPs)
     const T* sell_val_at = nullptr;
+    // FP64 phase reading the FP32 copy of the matrix (every scaled value exactly an FP32
+    // number): the same products and sums as with the FP64 copy, 4 bytes an entry less
+    bool compact = false;
+    const float* csr_val32 = nullptr;
+    const float* csc_val32 = nullptr;
+    const float* sell_val32_a = nullptr;
+    const float* sell_val32_at = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};   // around the first iteration of a chunk
@@ -394,23 +401,68 @@ struct Phase {
 // `timed`: bracket the two kernels with event-record nodes (captured into the chunk graph).
 // One SpMV of an iteration in shape v.group; the sliced-ELL shape reads its own copy of the
 // values (`sell_val`), every other shape the CSR-order ones.
+// VV: stored value type, T: vector and accumulation type.
+template <typename VV, typename T, class Epi>
+void launch_iter(const CsrView& v, const VV* csr_val, const VV* sell_val, const T* x, Epi epi, cudaStream_t st) {
+    if (v.group == kSell && v.sell_off && sell_val) launch_sell<VV, T, T>(v, csr_val, sell_val, x, epi, st);
+    else if (v.group == kSellHot && v.sell_off && sell_val) launch_sell_hot<VV, T, T>(v, csr_val, sell_val, x, epi, st);
+    else launch_spmv_t<VV, T, T>(v, csr_val, x, epi, st);
+}
+
+// The two iteration SpMVs of a phase, from the phase's copy of the values (A^T y: stored
+// transpose; A x: CSR).
 template <typename T, class Epi>
-void launch_iter(const CsrView& v, const T* csr_val, const T* sell_val, const T* x, Epi epi, cudaStream_t st) {
-    if (v.group == kSell && v.sell_off && sell_val) launch_sell<T, T, T>(v, csr_val, sell_val, x, epi, st);
-    else launch_spmv_t<T, T, T>(v, csr_val, x, epi, st);
+void phase_spmv_at(const Phase<T>& ph, const CsrView& v, const T* x, Epi epi, cudaStream_t st) {
+    if constexpr (sizeof(T) == 8) {
+        if (ph.compact) { launch_iter<float, T>(v, ph.csc_val32, ph.sell_val32_at, x, epi, st); return; }
+    }
+    launch_iter<T, T>(v, ph.csc_val, ph.sell_val_at, x, epi, st);
+}
+template <typename T, class Epi>
+void phase_spmv_a(const Phase<T>& ph, const CsrView& v, const T* x, Epi epi, cudaStream_t st) {
+    if constexpr (sizeof(T) == 8) {
+        if (ph.compact) { launch_iter<float, T>(v, ph.csr_val32, ph.sell_val32_a, x, epi, st); return; }
+    }
+    launch_iter<T, T>(v, ph.csr_val, ph.sell_val_a, x, epi, st);
+}
+
+// The check SpMVs of one phase (FP64 values -- or their exact FP32 copy -- and FP64 sums, the
+// phase's iterate type as the vector).
+template <typename VV, typename T>
+void launch_check_spmv(const CsrView& v, const VV* csr_val, const VV* sell_val, const T* x, double* out,
+                       const HState* S, int phase, cudaStream_t st) {
+    const EpiStoreActive epi{out, S, phase};
+    if (v.group == kSell && v.sell_off && sell_val) launch_sell<VV, T, double>(v, csr_val, sell_val, x, epi, st);
+    else if (v.group == kSellHot && v.sell_off && sell_val)
+        launch_sell_hot<VV, T, double>(v, csr_val, sell_val, x, epi, st);
+    else launch_spmv_t<VV, T, double>(v, csr_val, x, epi, st);
+}
+
+// Shared-memory grants of the hot-prefix kernels a phase may launch (outside any capture).
+template <typename T>
+vajra_status prepare_hot_kernels() {
+    VJ_CUDA((sell_hot_prepare<T, T, T, EpiHPrimal<T>>()));
+    VJ_CUDA((sell_hot_prepare<T, T, T, EpiHDual<T>>()));
+    VJ_CUDA((sell_hot_prepare<double, T, double, EpiStoreActive>()));
+    VJ_CUDA((sell_hot_prepare<float, T, double, EpiStoreActive>()));
+    if constexpr (sizeof(T) == 8) {
+        VJ_CUDA((sell_hot_prepare<float, T, T, EpiHPrimal<T>>()));
+        VJ_CUDA((sell_hot_prepare<float, T, T, EpiHDual<T>>()));
+    }
+    return VAJRA_OK;
 }
 
 template <typename T>
 void enqueue_iteration(Phase<T>& ph, const CsrView& a, const CsrView& at, HState* S, const double* hw, int kk,
                        int write_cand, bool timed, cudaStream_t st) {
     if (timed) cudaEventRecordWithFlags(ph.ev[0], st, cudaEventRecordExternal);
-    launch_iter<T>(at, ph.csc_val, ph.sell_val_at, ph.y.get(),
-                   EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                 ph.xc.get(), ph.xprev.get(), S, hw, kk, ph.phase, write_cand}, st);
+    phase_spmv_at(ph, at, ph.y.get(),
+                  EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
+                                ph.xc.get(), ph.xprev.get(), S, hw, kk, ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[1], st, cudaEventRecordExternal);
-    launch_iter<T>(a, ph.csr_val, ph.sell_val_a, ph.xb.get(),
-                   EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, kk,
-                               ph.phase, write_cand}, st);
+    phase_spmv_a(ph, a, ph.xb.get(),
+                 EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(), S, hw, kk,
+                             ph.phase, write_cand}, st);
     if (timed) cudaEventRecordWithFlags(ph.ev[2], st, cudaEventRecordExternal);
 }
 
@@ -418,22 +470,25 @@ struct CheckBuffers {
     DeviceBuffer<double> ax, aty, part_r, part_c, x_last, y_last;
     DeviceBuffer<double> hw;   // Halpern weights of the current chunk (2 per iteration)
     int hw_len = 0;            // iterations a chunk can hold
+    bool compact_checks = false;   // check SpMVs read the exact FP32 copy of the values
 };
 
 template <typename T>
 void enqueue_check(Phase<T>& ph, const CsrView& a64, const CsrView& at64, const Prepared& p, const DeviceLp& lp,
                    CheckBuffers& cb, HState* S, const ControlParams& cp, cudaStream_t st) {
-    // FP64 values of the scaled A; in sliced-ELL order too when that is the FP64 shape
-    if (a64.group == kSell && a64.sell_off)
-        launch_sell<double, T, double>(a64, p.csr_val.get(), p.sell_a.val64.get(), ph.xc.get(),
-                                       EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
-    else
-        launch_spmv_t<double, T, double>(a64, p.csr_val.get(), ph.xc.get(), EpiStoreActive{cb.ax.get(), S, ph.phase}, st);
-    if (at64.group == kSell && at64.sell_off)
-        launch_sell<double, T, double>(at64, p.csc_val.get(), p.sell_at.val64.get(), ph.yc.get(),
-                                       EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
-    else
-        launch_spmv_t<double, T, double>(at64, p.csc_val.get(), ph.yc.get(), EpiStoreActive{cb.aty.get(), S, ph.phase}, st);
+    // FP64 values of the scaled A (their FP32 copy where that is exact); in sliced-ELL order
+    // too when that is the FP64 shape
+    if (cb.compact_checks) {
+        launch_check_spmv<float, T>(a64, p.csr_val32.get(), p.sell_a.val32.get(), ph.xc.get(), cb.ax.get(), S,
+                                    ph.phase, st);
+        launch_check_spmv<float, T>(at64, p.csc_val32.get(), p.sell_at.val32.get(), ph.yc.get(), cb.aty.get(), S,
+                                    ph.phase, st);
+    } else {
+        launch_check_spmv<double, T>(a64, p.csr_val.get(), p.sell_a.val64.get(), ph.xc.get(), cb.ax.get(), S,
+                                     ph.phase, st);
+        launch_check_spmv<double, T>(at64, p.csc_val.get(), p.sell_at.val64.get(), ph.yc.get(), cb.aty.get(), S,
+                                     ph.phase, st);
+    }
     k_kkt_rows<T><<<kCheckBlocks, kThreads, 0, st>>>(ph.m, cb.ax.get(), ph.yc.get(), ph.yprev.get(), p.row_lower.get(), p.row_upper.get(),
                                                      lp.row_lower.get(), lp.row_upper.get(), p.row_scale.get(),
                                                      cb.y_last.get(), cb.part_r.get(), S, ph.phase);
@@ -481,8 +536,8 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
     auto time_shapes = [&](CsrView& v, auto launch) -> vajra_status {
         if (v.rows <= 0) return VAJRA_OK;
         constexpr int kFinal = 3;
-        int shapes[9] = {0, kRowblock2, 1, 2, 4, 8, 16, 32, kSell};
-        const int kShapes = v.sell_off ? 9 : 8;
+        int shapes[10] = {0, kRowblock2, 1, 2, 4, 8, 16, 32, kSell, kSellHot};
+        const int kShapes = v.sell_off ? 10 : 8;
         auto timed = [&](int g, int launches, float* ms) -> vajra_status {
             CsrView t = v;
             t.group = g;
@@ -493,14 +548,14 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
             VJ_CUDA(cudaEventElapsedTime(ms, e0, e1));
             return VAJRA_OK;
         };
-        float first[9];
+        float first[10];
         for (int i = 0; i < kShapes; ++i) {
             CsrView t = v;
             t.group = shapes[i];
             launch(t);   // warm
             VJ_TRY(timed(shapes[i], 3, &first[i]));
         }
-        int order[9];
+        int order[10];
         for (int i = 0; i < kShapes; ++i) order[i] = i;
         std::sort(order, order + kShapes, [&](int a, int b) { return first[a] < first[b]; });
         float total[kFinal] = {0.f, 0.f, 0.f};
@@ -517,14 +572,14 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
         return VAJRA_OK;
     };
     VJ_TRY(time_shapes(at, [&](const CsrView& t) {
-        launch_iter<T>(t, ph.csc_val, ph.sell_val_at, ph.y.get(),
-                       EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
-                                     ph.xc.get(), ph.xprev.get(), tune_state, hw, 0, ph.phase, 0}, st);
+        phase_spmv_at(ph, t, ph.y.get(),
+                      EpiHPrimal<T>{ph.c.get(), ph.cl.get(), ph.cu.get(), ph.x0.get(), ph.x.get(), ph.xb.get(),
+                                    ph.xc.get(), ph.xprev.get(), tune_state, hw, 0, ph.phase, 0}, st);
     }));
     VJ_TRY(time_shapes(a, [&](const CsrView& t) {
-        launch_iter<T>(t, ph.csr_val, ph.sell_val_a, ph.xb.get(),
-                       EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
-                                   tune_state, hw, 0, ph.phase, 0}, st);
+        phase_spmv_a(ph, t, ph.xb.get(),
+                     EpiHDual<T>{ph.rl.get(), ph.ru.get(), ph.y0.get(), ph.y.get(), ph.yc.get(), ph.yprev.get(),
+                                 tune_state, hw, 0, ph.phase, 0}, st);
     }));
     return VAJRA_OK;
 }
@@ -545,8 +600,9 @@ struct TuneKey {
     int device, m, n;
     int64_t nnz;
     int ordered;
+    int compact;
     bool operator<(const TuneKey& o) const {
-        return std::tie(device, m, n, nnz, ordered) < std::tie(o.device, o.m, o.n, o.nnz, o.ordered);
+        return std::tie(device, m, n, nnz, ordered, compact) < std::tie(o.device, o.m, o.n, o.nnz, o.ordered, o.compact);
     }
 };
 struct TuneEntry { int bits = 0, a32 = 8, at32 = 8, a64 = 8, at64 = 8; };
@@ -593,20 +649,29 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     so.ruiz_tolerance = 0.05;
     so.pock_chambolle = o.pock_chambolle != 0;
     so.negate_c = is_max;
+    so.pow2 = o.pow2_scaling != 0;
     VJ_TRY(prepare_scaled(lp, p, so, sst.get(), st));
     mark("scaling");
     VJ_TRY(plan_spmv(lp, p, st));
     mark("partitions");
-    if (mixed) VJ_TRY(make_f32_values(p, nnz, st));
+    // FP64 iterations and checks on the FP32 copy of the values where that copy is exact
+    const bool want_compact = o.fp64_value_storage == 2 || (o.fp64_value_storage == 0 && mixed);
+    bool compact = false;
+    if (want_compact) VJ_TRY(values_fit_fp32(p, nnz, &compact, st));
+    if (mixed || compact) VJ_TRY(make_f32_values(p, nnz, st));
     // Sliced-ELL copies of both matrices (full slices need rows of similar length, which the
     // degree ordering provides): one more launch shape for the autotuner, and the power
     // iteration's SpMVs.  Without the ordering they are built only when a caller forces the
     // shape.
-    if (ordered || o.spmv_shape_a == -3 || o.spmv_shape_at == -3) {
-        VJ_TRY(build_sell(p.a, p.csr_val.get(), mixed ? p.csr_val32.get() : nullptr, p.sell_a, st));
-        VJ_TRY(build_sell(p.at, p.csc_val.get(), mixed ? p.csc_val32.get() : nullptr, p.sell_at, st));
+    if (ordered || o.spmv_shape_a <= -3 || o.spmv_shape_at <= -3) {
+        VJ_TRY(build_sell(p.a, p.csr_val.get(), mixed || compact ? p.csr_val32.get() : nullptr, p.sell_a, st));
+        VJ_TRY(build_sell(p.at, p.csc_val.get(), mixed || compact ? p.csc_val32.get() : nullptr, p.sell_at, st));
     }
     mark("sliced ell");
+    if (p.a.sell_off || p.at.sell_off) {
+        if (mixed) VJ_TRY(prepare_hot_kernels<float>());
+        VJ_TRY(prepare_hot_kernels<double>());
+    }
     VJ_TRY(spectral_norm_fast(p, m, n, 100, 1e-5, sst.get(), st));
     mark("norm estimate");
     SetupState hss{};
@@ -648,6 +713,13 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     p64.csc_val = p.csc_val.get();
     p64.sell_val_a = p.a.sell_off ? p.sell_a.val64.get() : nullptr;
     p64.sell_val_at = p.at.sell_off ? p.sell_at.val64.get() : nullptr;
+    if (compact) {
+        p64.compact = true;
+        p64.csr_val32 = p.csr_val32.get();
+        p64.csc_val32 = p.csc_val32.get();
+        p64.sell_val32_a = p.a.sell_off ? p.sell_a.val32.get() : nullptr;
+        p64.sell_val32_at = p.at.sell_off ? p.sell_at.val32.get() : nullptr;
+    }
 
     mark("iterate buffers");
     CheckBuffers cb;
@@ -659,6 +731,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(cb.y_last.alloc(m));
     const int K = o.check_frequency > 0 ? o.check_frequency : 64;
     cb.hw_len = K;
+    cb.compact_checks = compact;
     VJ_TRY(cb.hw.alloc(2 * static_cast<size_t>(K)));
 
     HState init{};
@@ -693,7 +766,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     // Below ~1M entries a solve is launch-bound and the timing runs would cost more than any
     // shape saves: the set-up heuristic (lanes per row from the mean row length) stays.
     constexpr int64_t kAutotuneMinNnz = int64_t(1) << 20;
-    const TuneKey tkey{h->device, m, n, nnz, ordered ? 1 : 0};
+    const TuneKey tkey{h->device, m, n, nnz, ordered ? 1 : 0, compact ? 1 : 0};
     if (o.autotune) {   // shapes another handle already tuned for this LP
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cache.find(tkey);
@@ -743,6 +816,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             shape == 32)
             v32.group = v64.group = shape == -1 ? 0 : (shape == -2 ? kRowblock2 : shape);
         if (shape == -3) v32.group = v64.group = v32.sell_off ? kSell : 0;   // sliced ELL, else row block
+        if (shape == -4) v32.group = v64.group = v32.sell_off ? kSellHot : 0;   // ... with the hot prefix
     };
     forced(o.spmv_shape_a, a32, a64);
     forced(o.spmv_shape_at, at32, at64);
@@ -936,7 +1010,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     r->spmv_group_at = at_it.group;
     {
         const bool use32 = mixed && hs->phase_iters[0] >= hs->phase_iters[1];
-        const double vs = use32 ? 4.0 : 8.0;   // value / vector bytes
+        const double vs = use32 ? 4.0 : 8.0;                        // vector bytes
+        const double vb = (use32 || p64.compact) ? 4.0 : 8.0;       // matrix value bytes
         const double nn = static_cast<double>(nnz), dm = m, dn = n;
         const double t = use32 ? p32.t_primal_ms : p64.t_primal_ms, d = use32 ? p32.t_dual_ms : p64.t_dual_ms;
         const int64_t ns = use32 ? p32.samples : p64.samples;
@@ -946,8 +1021,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         // primal: CSC pointers (int64), indices + values, y gathered once, c/l/u/x/x0 read,
         // x and x_bar written.  dual: CSR pointers, indices + values, x_bar gathered once,
         // l/u/y/y0 read, y written.
-        r->primal_kernel_bytes = 8.0 * (dn + 1) + (4.0 + vs) * nn + vs * dm + 7.0 * vs * dn;
-        r->dual_kernel_bytes = 8.0 * (dm + 1) + (4.0 + vs) * nn + vs * dn + 5.0 * vs * dm;
+        r->primal_kernel_bytes = 8.0 * (dn + 1) + (4.0 + vb) * nn + vs * dm + 7.0 * vs * dn;
+        r->dual_kernel_bytes = 8.0 * (dm + 1) + (4.0 + vb) * nn + vs * dn + 5.0 * vs * dm;
     }
     const char* msg = status == kStatusOptimal ? "relative KKT tolerance reached"
                     : status == kStatusNumerical ? "NaN/Inf in the KKT evaluation"

@@ -87,6 +87,7 @@ struct ScalingOpts {
     double ruiz_tolerance = 0.05;
     bool pock_chambolle = false;
     bool negate_c = false;     // maximisation
+    bool pow2 = false;         // round the final factors to powers of two (exact scaling)
 };
 
 // Copies the raw data into the working buffers and applies Ruiz (exactly as
@@ -94,6 +95,9 @@ struct ScalingOpts {
 // fills the CSR-ordered values.  `sst` is a device SetupState.
 vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& o,
                             SetupState* sst, cudaStream_t st);
+
+// True when every scaled value is exactly representable in FP32 (one host synchronisation).
+vajra_status values_fit_fp32(const Prepared& p, int64_t nnz, bool* exact, cudaStream_t st);
 
 // f32 copies of the scaled values (mixed-precision path).
 vajra_status make_f32_values(Prepared& p, int64_t nnz, cudaStream_t st);

@@ -214,6 +214,24 @@ __global__ void k_row_abs_sum(int m, const int64_t* __restrict__ csr_ptr, const 
     out[i] = s;
 }
 
+// The cumulative factors rounded to the nearest power of two (in log2): scaling by them is
+// exact in binary floating point, so a matrix whose values fit FP32 still fits it after
+// scaling, and the scaled LP is the original one up to exact exponent shifts.
+__global__ void k_round_pow2(int64_t n, double* __restrict__ s) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double v = s[k];
+        if (v > 0.0 && isfinite(v)) s[k] = ldexp(1.0, static_cast<int>(rint(log2(v))));
+    }
+}
+
+// Raises *flag when a scaled value does not survive a round trip through FP32.
+__global__ void k_fp32_exact(int64_t nnz, const double* __restrict__ v, int* __restrict__ flag) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < nnz;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        if (static_cast<double>(static_cast<float>(v[k])) != v[k]) { *flag = 1; return; }
+}
+
 // c *= C; finite row bounds *= R; finite column bounds *= C^-1 (scaling.cpp:104-149).
 __global__ void k_scale_vectors(int m, int n, double* c, double* rl, double* ru, double* cl, double* cu,
                                 const double* __restrict__ rs, const double* __restrict__ cs) {
@@ -297,6 +315,17 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
             VJ_LAUNCH_CHECK();
             note_launch(5);
         }
+        if (o.pow2) {
+            // round the cumulative factors and scale the original values by them once
+            k_round_pow2<<<grid_stride_blocks(m), kThreads, 0, st>>>(m, p.row_scale.get());
+            k_round_pow2<<<grid_stride_blocks(n), kThreads, 0, st>>>(n, p.col_scale.get());
+            VJ_CUDA(cudaMemcpyAsync(p.csc_val.get(), lp.values.get(), sizeof(double) * nnz, cudaMemcpyDeviceToDevice, st));
+            k_scale_matrix<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, col_of.get(), lp.row_idx.get(),
+                                                                          p.csc_val.get(), p.row_scale.get(),
+                                                                          p.col_scale.get(), sst, 0);
+            VJ_LAUNCH_CHECK();
+            note_launch(3);
+        }
         const int mx = m > n ? m : n;
         k_scale_vectors<<<grid_for(mx), kThreads, 0, st>>>(m, n, p.c.get(), p.row_lower.get(), p.row_upper.get(),
                                                            p.col_lower.get(), p.col_upper.get(),
@@ -317,6 +346,22 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
     // CSR views: A over csr_*, A^T over the raw CSC structure.
     p.a.rows = m; p.a.cols = n; p.a.nnz = nnz; p.a.ptr = p.csr_ptr.get(); p.a.idx = p.csr_idx.get();
     p.at.rows = n; p.at.cols = m; p.at.nnz = nnz; p.at.ptr = lp.col_ptr.get(); p.at.idx = lp.row_idx.get();
+    return VAJRA_OK;
+}
+
+vajra_status values_fit_fp32(const Prepared& p, int64_t nnz, bool* exact, cudaStream_t st) {
+    *exact = false;
+    if (nnz <= 0) { *exact = true; return VAJRA_OK; }
+    DeviceBuffer<int> flag;
+    VJ_TRY(flag.alloc(1));
+    VJ_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), st));
+    k_fp32_exact<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, p.csc_val.get(), flag.get());
+    VJ_LAUNCH_CHECK();
+    note_launch(1);
+    int h = 1;
+    VJ_CUDA(cudaMemcpyAsync(&h, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
+    *exact = h == 0;
     return VAJRA_OK;
 }
 

@@ -21,6 +21,8 @@
 // The autotuner of each solver picks the family and shape per matrix and precision.
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace vajra {
@@ -359,9 +361,24 @@ template <typename T> struct Pack2;
 template <> struct Pack2<float> { using type = float2; };
 template <> struct Pack2<double> { using type = double2; };
 
-template <typename VV, typename VX, typename Acc, class Epi>
+// Where a kernel reads the dense vector's entries from: global memory through the read-only
+// path, or -- for the entries [0, hot) of the hot-prefix kernel -- a copy in shared memory.
+template <typename VX>
+struct GatherGlobal {
+    const VX* __restrict__ x;
+    __device__ __forceinline__ VX operator()(int j) const { return ld_cached(x + j); }
+};
+template <typename VX>
+struct GatherHot {
+    const VX* __restrict__ x;
+    const VX* xs;   // shared-memory copy of x[0, hot)
+    int hot;
+    __device__ __forceinline__ VX operator()(int j) const { return j < hot ? xs[j] : ld_cached(x + j); }
+};
+
+template <typename VV, typename VX, typename Acc, class Epi, class G>
 __device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                              const VV* __restrict__ val, const VX* __restrict__ x, const Epi& epi) {
+                                              const VV* __restrict__ val, const G& gx, const Epi& epi) {
     const int lane = threadIdx.x & 31;
     PreOf<Epi> pre{};
     if (lane == 0) pre = epi_pre(epi, row, 0);
@@ -369,7 +386,7 @@ __device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict
     Acc acc = Acc(0);
 #pragma unroll 4
     for (int64_t k = s + lane; k < e; k += 32)
-        acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(ld_cached(x + ld_stream(idx + k))), acc);
+        acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(gx(ld_stream(idx + k))), acc);
     acc = warp_reduce<OpSum>(acc);
     if (lane == 0) epi_fin(epi, row, acc, pre, 0);
 }
@@ -380,10 +397,10 @@ __device__ __forceinline__ void sell_warp_row(int row, const int64_t* __restrict
 constexpr uint8_t kSellLong = 0xFF;
 static_assert(kSellWidth < kSellLong, "row lengths of the slices must fit one byte below the marker");
 
-template <typename VV, typename VX, typename Acc, class Epi>
+template <typename VV, typename VX, typename Acc, class Epi, class G>
 __device__ __forceinline__ void sell_slice(int sl, int rows, const uint8_t* __restrict__ sell_len,
                                            const int64_t* __restrict__ sell_off, const int32_t* __restrict__ sell_idx,
-                                           const VV* __restrict__ sell_val, const VX* __restrict__ x, const Epi& epi) {
+                                           const VV* __restrict__ sell_val, const G& gx, const Epi& epi) {
     const int lane = threadIdx.x & 31;
     const int row = sl * 32 + lane;
     if (row >= rows) return;
@@ -396,8 +413,7 @@ __device__ __forceinline__ void sell_slice(int sl, int rows, const uint8_t* __re
 #pragma unroll 4
         for (int k = 0; k < len; ++k) {
             const int64_t q = base + 32 * static_cast<int64_t>(k);
-            acc = fma(static_cast<Acc>(ld_stream(sell_val + q)), static_cast<Acc>(ld_cached(x + ld_stream(sell_idx + q))),
-                      acc);
+            acc = fma(static_cast<Acc>(ld_stream(sell_val + q)), static_cast<Acc>(gx(ld_stream(sell_idx + q))), acc);
         }
     } else {
         // one 8-byte index load and one 8- or 16-byte value load per pair (the slot after an
@@ -410,8 +426,8 @@ __device__ __forceinline__ void sell_slice(int sl, int rows, const uint8_t* __re
             const int64_t q = base + 64 * static_cast<int64_t>(j);
             const int2 ii = __ldcs(reinterpret_cast<const int2*>(sell_idx + q));
             const VV2 vv = __ldcs(reinterpret_cast<const VV2*>(sell_val + q));
-            acc = fma(static_cast<Acc>(vv.x), static_cast<Acc>(ld_cached(x + ii.x)), acc);
-            if (2 * j + 1 < len) acc = fma(static_cast<Acc>(vv.y), static_cast<Acc>(ld_cached(x + ii.y)), acc);
+            acc = fma(static_cast<Acc>(vv.x), static_cast<Acc>(gx(ii.x)), acc);
+            if (2 * j + 1 < len) acc = fma(static_cast<Acc>(vv.y), static_cast<Acc>(gx(ii.y)), acc);
         }
     }
     epi_fin(epi, row, acc, pre, 0);
@@ -451,12 +467,66 @@ k_spmv_sell(int rows, int slices, const int64_t* __restrict__ ptr, const int32_t
         const int w = b * kWarps + warp;
         if (w < n_long) {
             const int row = long_rows[w];
-            if (!skip_rows_impl(epi, row, row + 1, 0)) sell_warp_row<VV, VX, Acc>(row, ptr, idx, val, x, epi);
+            if (!skip_rows_impl(epi, row, row + 1, 0))
+                sell_warp_row<VV, VX, Acc>(row, ptr, idx, val, GatherGlobal<VX>{x}, epi);
         }
         return;
     }
     const int sl = (b - long_ctas) * kWarps + warp;
-    if (sl < slices) sell_slice<VV, VX, Acc>(sl, rows, sell_len, sell_off, sell_idx, sell_val, x, epi);
+    if (sl < slices) sell_slice<VV, VX, Acc>(sl, rows, sell_len, sell_off, sell_idx, sell_val, GatherGlobal<VX>{x}, epi);
+}
+
+// ----- sliced ELL with the hot prefix of the dense vector in shared memory ---------------
+// On the degree-ordered LP the vector entries gathered most often are the first ones: the
+// 28,672 longest columns of the 1M x 2M LP hold 40 % of A's entries.  Every CTA of this
+// persistent kernel first copies x[0, hot) into shared memory, and the gathers below `hot` are
+// then served from there -- a shared-memory access instead of an L1/L2 request, which is
+// what bounds the plain kernel.  Persistent CTAs (kSellHotCtasPerSm per SM, kSellHotThreads
+// threads) amortise the copy; the CTAs walk the very long rows (one CTA each), then their
+// warps take the listed long rows and the slices in an interleaved order (slice widths fall
+// along the order, so interleaving balances the warps).  Sums and epilogues are the plain
+// kernel's, so results are bit-identical to it.
+constexpr int kSellHotThreads = 768;
+constexpr int kSellHotCtasPerSm = 2;
+constexpr int kSellHotBytes = 112 * 1024;   // shared memory per CTA (two CTAs fill an SM's 228 KB)
+
+template <typename VV, typename VX, typename Acc, class Epi>
+__global__ void __launch_bounds__(kSellHotThreads, kSellHotCtasPerSm)
+k_spmv_sell_hot(int rows, int slices, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                const VV* __restrict__ val, const int32_t* __restrict__ vlong_rows, int n_vlong,
+                const int32_t* __restrict__ long_rows, int n_long, const uint8_t* __restrict__ sell_len,
+                const int64_t* __restrict__ sell_off, const int32_t* __restrict__ sell_idx,
+                const VV* __restrict__ sell_val, const VX* __restrict__ x, int hot, Epi epi) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Acc red[32];
+    VX* xs = reinterpret_cast<VX*>(smem_raw);
+    if (!epi.active()) return;   // uniform over the grid (device state)
+    // x[0, hot): 16-byte loads (x is a device allocation, 256-byte aligned; hot is a multiple
+    // of the vector width), written by the previous kernel, so a plain load
+    constexpr int kVec = 16 / sizeof(VX);
+    for (int k = threadIdx.x * kVec; k < hot; k += kSellHotThreads * kVec) {
+        if constexpr (sizeof(VX) == 4) *reinterpret_cast<float4*>(xs + k) = *reinterpret_cast<const float4*>(x + k);
+        else *reinterpret_cast<double2*>(xs + k) = *reinterpret_cast<const double2*>(x + k);
+    }
+    __syncthreads();
+    const GatherHot<VX> gx{x, xs, hot};
+    for (int i = blockIdx.x; i < n_vlong; i += gridDim.x) {   // uniform over the CTA
+        const int row = vlong_rows[i];
+        const int64_t s = ptr[row], e = ptr[row + 1];
+        Acc acc = Acc(0);
+        for (int64_t k = s + threadIdx.x; k < e; k += kSellHotThreads)
+            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(gx(ld_stream(idx + k))), acc);
+        Acc v[1] = {acc};
+        block_reduce<OpSum, Acc, 1>(v, red);
+        if (threadIdx.x == 0) epi(row, v[0]);
+    }
+    constexpr int kWarps = kSellHotThreads / 32;
+    const int warp = static_cast<int>(threadIdx.x >> 5);
+    const int items = n_long + slices;
+    for (int w = blockIdx.x * kWarps + warp; w < items; w += gridDim.x * kWarps) {
+        if (w < n_long) sell_warp_row<VV, VX, Acc>(long_rows[w], ptr, idx, val, gx, epi);
+        else sell_slice<VV, VX, Acc>(w - n_long, rows, sell_len, sell_off, sell_idx, sell_val, gx, epi);
+    }
 }
 
 // Host-side description of one SpMV operand (a CSR, possibly the stored transpose) and the
@@ -513,6 +583,46 @@ inline void launch_sell(const CsrView& a, const VV* csr_val, const VV* sell_val,
     note_launch();
 }
 
+// Launch-shape code of the hot-prefix sliced-ELL kernel.
+constexpr int kSellHot = 129;
+
+// Streaming multiprocessors of the current device (read once per device).
+int sm_count();
+
+// Entries of the dense vector the hot-prefix kernel keeps in shared memory.
+template <typename VX>
+inline int sell_hot_extent(int cols) {
+    const int cap = kSellHotBytes / static_cast<int>(sizeof(VX));
+    return cols < cap ? (cols + 3) / 4 * 4 : cap;   // a multiple of four: whole 16-byte loads
+}
+
+// The kernel needs more than 48 KB of dynamic shared memory, which is granted per kernel and
+// device.  Called outside any stream capture (the solver's set-up does) before the first
+// launch; idempotent.
+template <typename VV, typename VX, typename Acc, class Epi>
+inline cudaError_t sell_hot_prepare() {
+    return cudaFuncSetAttribute(k_spmv_sell_hot<VV, VX, Acc, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kSellHotBytes);
+}
+
+template <typename VV, typename VX, typename Acc, class Epi>
+inline void launch_sell_hot(const CsrView& a, const VV* csr_val, const VV* sell_val, const VX* x, Epi epi,
+                            cudaStream_t st) {
+    constexpr int kWarps = kSellHotThreads / 32;
+    const int items = a.sell_n_long + a.sell_slices;
+    int grid = sm_count() * kSellHotCtasPerSm;
+    const int need = std::max(a.sell_n_vlong, (items + kWarps - 1) / kWarps);
+    if (need < grid) grid = need;
+    if (grid <= 0) return;
+    const int hot = sell_hot_extent<VX>(a.cols);
+    // a vector shorter than the 16-byte padding of its allocation is still read whole (the
+    // buffers carry 16 spare elements, so the rounded-up extent stays inside the allocation)
+    k_spmv_sell_hot<VV, VX, Acc, Epi><<<grid, kSellHotThreads, static_cast<size_t>(hot) * sizeof(VX), st>>>(
+        a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
+        a.sell_n_long, a.sell_len, a.sell_off, a.sell_idx, sell_val, x, hot, epi);
+    note_launch();
+}
+
 // Launch-shape code of the row-block kernel with two groups of four entries in flight per
 // thread (U = 2).  With 4-byte values it keeps six CTAs per SM by leaving the epilogue's loads
 // to the end (they would not fit in 40 registers); with 8-byte values it keeps them early at
@@ -550,6 +660,7 @@ inline void launch_spmv_t(const CsrView& a, const VV* val, const VX* x, Epi epi,
     if (a.rows <= 0) return;
     switch (a.group) {
         case kSell:
+        case kSellHot:
         case 0:
             if (a.tiles) { launch_rowblock<VV, VX, Acc, 1>(a, val, x, epi, st); break; }
             launch_vec_g<VV, VX, Acc, 8>(a, val, x, epi, st);

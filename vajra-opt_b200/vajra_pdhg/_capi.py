@@ -16,12 +16,12 @@ _fp = C.POINTER(C.c_float)
 _i64p = C.POINTER(C.c_int64)
 _i32p = C.POINTER(C.c_int32)
 
-ABI_VERSION = 7   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
+ABI_VERSION = 8   # VAJRA_ABI_VERSION of include/vajra_pdhg.h these declarations follow
 
 # vajra_status
 OK, ERR_INVALID_ARGUMENT, ERR_NO_DEVICE, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_WAIT_TIMEOUT, ERR_INTERNAL = range(7)
 ALGO_REFERENCE, ALGO_HALPERN = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2   # PREC_FP32: vajra_pdhg_unrolled only
 
 
 class VajraLp(C.Structure):
@@ -43,7 +43,8 @@ class VajraOpts(C.Structure):
                 ("restart_artificial", C.c_double), ("primal_weight_smoothing", C.c_double),
                 ("step_safety", C.c_double), ("restart_metric", C.c_int32),
                 ("spmv_shape_a", C.c_int32), ("spmv_shape_at", C.c_int32),
-                ("mixed_reflection", C.c_double), ("degree_order", C.c_int32), ("reserved", C.c_int32)]
+                ("mixed_reflection", C.c_double), ("degree_order", C.c_int32), ("pow2_scaling", C.c_int32),
+                ("fp64_value_storage", C.c_int32), ("reserved", C.c_int32)]
 
 
 class VajraResult(C.Structure):

@@ -1,10 +1,16 @@
-"""Gradient harness for the adjoint of the unrolled PDHG map (vajra_pdhg_unrolled).
+"""Gradient harnesses: the adjoint of the unrolled PDHG map (vajra_pdhg_unrolled) and the
+gradient of the optimal value at a converged solution.
 
 `unrolled(lps, weights, ...)` calls the C ABI directly.  `UnrolledLoss` is a thin
 torch.autograd.Function around it: forward returns the per-instance losses
 L_i = sum_j (w_j + c_j) x_j(K), backward applies the device adjoint's dL/dc and dL/db (for
-equality rows b = row_lower = row_upper, so dL/db = dL/drow_lower + dL/drow_upper).  torch is
-used only to carry tensors through autograd; all arithmetic runs in libvajra_pdhg.so.
+equality rows b = row_lower = row_upper, so dL/db = dL/drow_lower + dL/drow_upper).
+
+`OptimalValue` differentiates V(c, b) = min {c.x : A x = b, l <= x <= u} itself: forward solves
+each LP to a tight FP64 relative KKT with the restarted Halpern solver, backward returns the
+envelope-theorem gradient dV/dc = x*, dV/db = y* (the row dual in the verifier's convention,
+col_dual = c - A^T y), which is exact wherever the optimal basis is unique.  torch is used only
+to carry tensors through autograd; all arithmetic runs in libvajra_pdhg.so.
 """
 from __future__ import annotations
 
@@ -13,7 +19,7 @@ import ctypes as C
 import numpy as np
 
 from . import _capi, _HostLp
-from ._capi import PREC_FP64, PREC_MIXED
+from ._capi import PREC_FP32, PREC_FP64, PREC_MIXED
 
 
 class VajraUnrolledOpts(C.Structure):
@@ -98,7 +104,42 @@ try:
             gc = ctx.grad_c * g[ctx.col_inst]
             gb = ctx.grad_b * g[ctx.row_inst]
             return gc, gb, None, None, None
+
+    class OptimalValue(torch.autograd.Function):
+        """V_i(c, b) per instance for equality-constrained LPs sharing A and bounds with
+        `templates`; backward: dV/dc = x*, dV/db = y* at the solutions forward found."""
+
+        @staticmethod
+        def forward(ctx, c, b, templates, solve_opts):
+            from . import solve
+            cs = c.detach().cpu().double().numpy()
+            bs = b.detach().cpu().double().numpy()
+            vals, xs, ys, co, ro = [], [], [], 0, 0
+            opts = {"precision": PREC_FP64, "tolerance": 1e-10, **(solve_opts or {})}
+            for t in templates:
+                r = solve(_with_cb(t, cs[co:co + t.num_cols], bs[ro:ro + t.num_rows]), **opts)
+                if r["status_name"] != "OPTIMAL":
+                    raise RuntimeError(f"OptimalValue: instance solve ended {r['status_name']}")
+                vals.append(r["objective_value"])
+                xs.append(r["x"])
+                ys.append(r["y"])
+                co += t.num_cols
+                ro += t.num_rows
+            ctx.x = torch.from_numpy(np.concatenate(xs))
+            ctx.y = torch.from_numpy(np.concatenate(ys))
+            ctx.col_inst = torch.repeat_interleave(torch.arange(len(templates)),
+                                                   torch.tensor([t.num_cols for t in templates]))
+            ctx.row_inst = torch.repeat_interleave(torch.arange(len(templates)),
+                                                   torch.tensor([t.num_rows for t in templates]))
+            return torch.tensor(vals, dtype=torch.float64).to(c.device)
+
+        @staticmethod
+        def backward(ctx, g):
+            g = g.detach().cpu().double()
+            return ctx.x * g[ctx.col_inst], ctx.y * g[ctx.row_inst], None, None
 except ImportError:  # torch is optional for the C-level API above
     UnrolledLoss = None
+    OptimalValue = None
 
-__all__ = ["unrolled", "UnrolledLoss", "default_unrolled_opts", "PREC_FP64", "PREC_MIXED"]
+__all__ = ["unrolled", "UnrolledLoss", "OptimalValue", "default_unrolled_opts", "PREC_FP64", "PREC_MIXED",
+           "PREC_FP32"]
