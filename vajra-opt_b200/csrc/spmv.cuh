@@ -368,12 +368,29 @@ struct GatherGlobal {
     const VX* __restrict__ x;
     __device__ __forceinline__ VX operator()(int j) const { return ld_cached(x + j); }
 };
+// Global load through the read-only path that only the lanes with `pred` issue (predicated
+// in PTX, so no branch splits the warp and the loads of an unrolled loop stay in flight
+// together); the other lanes keep `v`.
+__device__ __forceinline__ void ld_nc_if(float& v, const float* p, bool pred) {
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q ld.global.nc.f32 %0, [%1];\n\t}"
+        : "+f"(v) : "l"(p), "r"(static_cast<int>(pred)));
+}
+__device__ __forceinline__ void ld_nc_if(double& v, const double* p, bool pred) {
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %2, 0;\n\t@q ld.global.nc.f64 %0, [%1];\n\t}"
+        : "+d"(v) : "l"(p), "r"(static_cast<int>(pred)));
+}
 template <typename VX>
 struct GatherHot {
     const VX* __restrict__ x;
     const VX* xs;   // shared-memory copy of x[0, hot)
     int hot;
-    __device__ __forceinline__ VX operator()(int j) const { return j < hot ? xs[j] : ld_cached(x + j); }
+    __device__ __forceinline__ VX operator()(int j) const {
+        const bool cold = j >= hot;
+        VX g = VX(0);
+        ld_nc_if(g, x + j, cold);             // only the cold lanes make an L1/L2 request
+        const VX s = xs[cold ? 0 : j];        // every lane reads shared memory (cold lanes: entry 0)
+        return cold ? g : s;
+    }
 };
 
 template <typename VV, typename VX, typename Acc, class Epi, class G>
@@ -514,8 +531,11 @@ k_spmv_sell_hot(int rows, int slices, const int64_t* __restrict__ ptr, const int
         const int row = vlong_rows[i];
         const int64_t s = ptr[row], e = ptr[row + 1];
         Acc acc = Acc(0);
-        for (int64_t k = s + threadIdx.x; k < e; k += kSellHotThreads)
-            acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(gx(ld_stream(idx + k))), acc);
+        // the plain kernel's split of the row over kThreads threads (the other warps add zeros),
+        // so that the row sum has the same bits
+        if (threadIdx.x < kThreads)
+            for (int64_t k = s + threadIdx.x; k < e; k += kThreads)
+                acc = fma(static_cast<Acc>(ld_stream(val + k)), static_cast<Acc>(gx(ld_stream(idx + k))), acc);
         Acc v[1] = {acc};
         block_reduce<OpSum, Acc, 1>(v, red);
         if (threadIdx.x == 0) epi(row, v[0]);
