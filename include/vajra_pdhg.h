@@ -129,7 +129,8 @@ typedef struct vajra_opts {
                                    entries) or the set-up heuristic, -1 row-block kernel,
                                    -2 row-block kernel with two load groups per thread,
                                    -3 sliced ELL (degree-ordered LPs; else the row-block
-                                   kernel), 1..32 lanes per row (1, 2, 4, 8, 16, 32)        */
+                                   kernel), -4 sliced ELL with the first vector entries in
+                                   shared memory, 1..32 lanes per row (1, 2, 4, 8, 16, 32)   */
     int32_t spmv_shape_at;      /* the same for the A^T y SpMV                           */
     double mixed_reflection;    /* MIXED: reflection coefficient of the FP32 phase once its
                                    relative KKT is within 10x of mixed_switch_tolerance (0.8);
@@ -151,6 +152,12 @@ typedef struct vajra_opts {
                                    on when exact; FP64 form: off), 1 FP64 copy always, 2 the
                                    FP32 copy when exact in either precision                  */
     int32_t reserved;
+    double max_violation;       /* HALPERN: > 0 also requires, before OPTIMAL, the maxima that
+                                   the engine's status guard checks (Solution::recompute_quality,
+                                   src/engine/model.cpp:203-374) to be at most this on the
+                                   original LP: each row violation over 1 + |its bound|, each
+                                   reduced-cost sign violation of a column off its bound, each
+                                   row-dual sign violation (0 = relative KKT only)          */
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and
@@ -164,7 +171,9 @@ typedef struct vajra_result {
     int64_t iterations;
     double objective_value;
     double dual_objective;
-    /* PdhgDiagnostics surface (include/indus/pdhg.hpp:30-43) */
+    /* PdhgDiagnostics surface (include/indus/pdhg.hpp:30-43); HALPERN reports as the residuals
+     * the largest absolute row violation and the largest reduced-cost / row-dual sign
+     * violation on the original LP (the status guard's quantities) */
     int32_t restart_count;
     double primal_residual;
     double dual_residual;
@@ -190,7 +199,8 @@ typedef struct vajra_result {
     int64_t host_device_transfers;
     int32_t spmv_group_a;       /* SpMV shape chosen for A x: 1..32 lanes per row, 0 the
                                    shared-memory row-block kernel, 64 the same with two load
-                                   groups per thread, 128 sliced ELL, -1 the exact in-order
+                                   groups per thread, 128 sliced ELL, 129 sliced ELL with the
+                                   hot vector prefix in shared memory, -1 the exact in-order
                                    kernel of VAJRA_ALGO_REFERENCE                            */
     int32_t spmv_group_at;      /* same for A^T y                                           */
     /* Live kernel timing (HALPERN): CUDA-event durations of the fused iteration kernels,

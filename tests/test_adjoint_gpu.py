@@ -128,14 +128,18 @@ def test_autograd_function(cuda):
 
 
 @pytest.mark.skipif(not B.ref_available(), reason="needs the reference's dual simplex (oracle/_ref)")
-@pytest.mark.parametrize("m,n,seed", [(60, 150, 44), (200, 500, 45)])
-def test_optimal_value_gradient_matches_simplex_duals(cuda, m, n, seed):
+@pytest.mark.parametrize("m,n,k,seed", [(60, 150, 5, 44), (200, 500, 8, 47)])
+def test_optimal_value_gradient_matches_simplex_duals(cuda, m, n, k, seed):
     """dV/db of V(c, b) = min c.x (the OptimalValue harness: the restarted Halpern solver to
     FP64 relative KKT 1e-10, envelope-theorem backward) against the reference dual simplex's
-    y* (src/engine/model.cpp:528-614) to 1e-4, and against central differences of V itself."""
+    y* (src/engine/model.cpp:528-614) to 1e-4, and against central differences of V itself.
+    y* is unique when the columns strictly between their bounds at the planted optimum have
+    full row rank (checked first: otherwise two correct solvers may return different duals)."""
     import torch
     from vajra_pdhg.autograd import OptimalValue
-    lp = W.random_planted(m, n, 5, seed=seed)
+    lp = W.random_planted(m, n, k, seed=seed)
+    interior = (lp.x_planted > 1e-9) & (lp.x_planted < 10 - 1e-9)
+    assert np.linalg.matrix_rank(lp.to_scipy_csc()[:, np.flatnonzero(interior)].toarray()) == m
     s = B.ref_solve(lp, algorithm="dual_simplex", through_solve=True, iteration_limit=100000)
     assert s["status_name"] == "OPTIMAL"
     c = torch.tensor(lp.c, dtype=torch.float64, requires_grad=True)

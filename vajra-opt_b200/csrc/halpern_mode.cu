@@ -30,14 +30,28 @@
 namespace vajra {
 namespace {
 
-constexpr int kQ = 7;             // partial sums per block in the check passes (last: NaN flag)
+// Per block of a check pass: kNS partial sums, then kNM maxima (NaN flag, then the status
+// guard's violation maxima of Solution::recompute_quality, src/engine/model.cpp:203-374).
+constexpr int kNS = 6;
+constexpr int kNM = 4;
+constexpr int kQ = kNS + kNM;
 constexpr int kCheckBlocks = 148 * 4;
+constexpr double kGuardTol = 1e-7;   // tol::kPrimalFeasibility / kDualFeasibility of the guard
 
 __device__ __forceinline__ bool finite_lo(double l) { return l > -1e20; }
 __device__ __forceinline__ bool finite_up(double u) { return u < 1e20; }
 
+__device__ __forceinline__ void store_partials(double (&v)[kQ], double* red, double* part) {
+    block_reduce<OpSum, double, kNS>(*reinterpret_cast<double(*)[kNS]>(v), red);
+    block_reduce<OpMax, double, kNM>(*reinterpret_cast<double(*)[kNM]>(v + kNS), red);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < kQ; ++q) part[blockIdx.x * kQ + q] = v[q];
+}
+
 // Row pass: original- and scaled-space primal residual, row part of the dual objective,
-// distance of y+ from the last restart point, NaN detection.
+// distance of y+ from the last restart point, NaN detection, and the guard's maxima: the
+// row violation relative to 1 + |violated bound|, its absolute size, and the row dual's sign
+// violation (verifier convention: y <= 0 on a <= row, y >= 0 on a >= row).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const T* __restrict__ yprev,
@@ -46,38 +60,43 @@ k_kkt_rows(int m, const double* __restrict__ ax, const T* __restrict__ yc, const
            double* __restrict__ part, const HState* st, int phase) {
     if (st->stop || st->phase != phase) return;
     __shared__ double red[kQ * 32];
-    double v[kQ] = {0, 0, 0, 0, 0, 0, 0};   // rp_o^2, rp_s^2, dobj, dy^2 (restart), dy^2 (step), -, nan
+    // sums: rp_o^2, rp_s^2, dobj, dy^2 (restart), dy^2 (step), -; maxima: nan, p_rel, p_abs, d_abs
+    double v[kQ] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         const double a = ax[i];
         const double ys = static_cast<double>(yc[i]);
-        if (!isfinite(a) || !isfinite(ys)) v[kQ - 1] = 1.0;
+        if (!isfinite(a) || !isfinite(ys)) v[kNS] = 1.0;
         const double fy = ys - static_cast<double>(yprev[i]);
         v[4] += fy * fy;
         const double ps = a - fmin(fmax(a, rl_s[i]), ru_s[i]);
         const double ao = a / rs[i];
-        const double po = ao - fmin(fmax(ao, rl_o[i]), ru_o[i]);
+        const double lo = rl_o[i], up = ru_o[i];
+        const double po = ao - fmin(fmax(ao, lo), up);
         const double yo = -ys * rs[i];          // verifier sign, original space
         double dt = 0.0;
-        if (yo > 0.0 && finite_lo(rl_o[i])) dt = yo * rl_o[i];
-        else if (yo < 0.0 && finite_up(ru_o[i])) dt = yo * ru_o[i];
+        if (yo > 0.0 && finite_lo(lo)) dt = yo * lo;
+        else if (yo < 0.0 && finite_up(up)) dt = yo * up;
         const double dy = ys - y_last[i];
         v[0] += po * po;
         v[1] += ps * ps;
         v[2] += dt;
         v[3] += dy * dy;
+        if (po != 0.0) {
+            const double bound = po < 0.0 ? (lo > -1e19 ? fabs(lo) : 1.0) : (up < 1e19 ? fabs(up) : 1.0);
+            v[kNS + 1] = fmax(v[kNS + 1], fabs(po) / (1.0 + bound));
+            v[kNS + 2] = fmax(v[kNS + 2], fabs(po));
+        }
+        if (!finite_lo(lo) && finite_up(up) && yo > 0.0) v[kNS + 3] = fmax(v[kNS + 3], yo);
+        if (finite_lo(lo) && !finite_up(up) && yo < 0.0) v[kNS + 3] = fmax(v[kNS + 3], -yo);
     }
-    block_reduce<OpSum, double, kQ - 1>(*reinterpret_cast<double(*)[kQ - 1]>(v), red);
-    double f[1] = {v[kQ - 1]};
-    block_reduce<OpMax, double, 1>(f, red);
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < kQ - 1; ++q) part[blockIdx.x * kQ + q] = v[q];
-        part[blockIdx.x * kQ + kQ - 1] = f[0];
-    }
+    store_partials(v, red, part);
 }
 
 // Column pass: reduced cost r = c + A^T y (min form), its bound-multiplier part lambda,
 // dual residual r - lambda (original and scaled), primal objective, column part of the dual
-// objective, distance of x+ from the last restart point.
+// objective, distance of x+ from the last restart point, and the guard's reduced-cost sign
+// violation (a column more than 1e-7 below its upper bound may not have r < 0, one more than
+// 1e-7 above its lower bound may not have r > 0).
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_kkt_cols(int n, const double* __restrict__ aty, const T* __restrict__ xc, const T* __restrict__ xprev,
@@ -86,36 +105,35 @@ k_kkt_cols(int n, const double* __restrict__ aty, const T* __restrict__ xc, cons
            const HState* st, int phase) {
     if (st->stop || st->phase != phase) return;
     __shared__ double red[kQ * 32];
-    double v[kQ] = {0, 0, 0, 0, 0, 0, 0};   // rd_o^2, rd_s^2, pobj, dobj, dx^2 (restart), dx^2 (step), nan
+    // sums: rd_o^2, rd_s^2, pobj, dobj, dx^2 (restart), dx^2 (step); maxima: nan, -, -, d_abs
+    double v[kQ] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const double at = aty[j];
         const double xs = static_cast<double>(xc[j]);
-        if (!isfinite(at) || !isfinite(xs)) v[kQ - 1] = 1.0;
+        if (!isfinite(at) || !isfinite(xs)) v[kNS] = 1.0;
         const double fx = xs - static_cast<double>(xprev[j]);
         v[5] += fx * fx;
-        const bool lf = finite_lo(cl_o[j]), uf = finite_up(cu_o[j]);
+        const double lo = cl_o[j], up = cu_o[j];
+        const bool lf = finite_lo(lo), uf = finite_up(up);
         const double r_s = c_s[j] + at;
         const double r_o = r_s / cs[j];
         auto lam_of = [&](double r) { return (lf && uf) ? r : lf ? fmax(r, 0.0) : uf ? fmin(r, 0.0) : 0.0; };
-        const double lo = lam_of(r_o), ls = lam_of(r_s);
-        const double ro = r_o - lo, rsd = r_s - ls;
+        const double lo_lam = lam_of(r_o), ls = lam_of(r_s);
+        const double ro = r_o - lo_lam, rsd = r_s - ls;
         double dt = 0.0;
-        if (lo > 0.0) dt = lo * cl_o[j];
-        else if (lo < 0.0) dt = lo * cu_o[j];
+        if (lo_lam > 0.0) dt = lo_lam * lo;
+        else if (lo_lam < 0.0) dt = lo_lam * up;
         const double dx = xs - x_last[j];
         v[0] += ro * ro;
         v[1] += rsd * rsd;
         v[2] += c_s[j] * xs;
         v[3] += dt;
         v[4] += dx * dx;
+        const double xo = xs * cs[j];
+        if (xo < up - kGuardTol && r_o < 0.0) v[kNS + 3] = fmax(v[kNS + 3], -r_o);
+        if (xo > lo + kGuardTol && r_o > 0.0) v[kNS + 3] = fmax(v[kNS + 3], r_o);
     }
-    block_reduce<OpSum, double, kQ - 1>(*reinterpret_cast<double(*)[kQ - 1]>(v), red);
-    double f[1] = {v[kQ - 1]};
-    block_reduce<OpMax, double, 1>(f, red);
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < kQ - 1; ++q) part[blockIdx.x * kQ + q] = v[q];
-        part[blockIdx.x * kQ + kQ - 1] = f[0];
-    }
+    store_partials(v, red, part);
 }
 
 struct ControlParams {
@@ -133,9 +151,10 @@ struct ControlParams {
     int mixed;        // 1 when an FP32 phase hands over to FP64
     int stall_checks; // FP32 stall window in checks (0 = no stall test; at most kHist - 1)
     int metric;       // restart metric: 0 weighted KKT, 1 fixed-point residual
+    double max_violation;   // > 0: also require the guard's maxima below this
 };
 
-constexpr int kS = 2 * (kQ - 1);   // sums the control CTA combines (rows, then columns)
+constexpr int kS = 2 * kNS;   // sums the control CTA combines (rows, then columns)
 
 __global__ void __launch_bounds__(1024)
 k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ part_c, ControlParams cp,
@@ -146,16 +165,24 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
 #pragma unroll
     for (int q = 0; q < kS; ++q) s[q] = 0.0;
     for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x) {
-        for (int q = 0; q < kQ - 1; ++q) { s[q] += part_r[b * kQ + q]; s[kQ - 1 + q] += part_c[b * kQ + q]; }
+        for (int q = 0; q < kNS; ++q) { s[q] += part_r[b * kQ + q]; s[kNS + q] += part_c[b * kQ + q]; }
     }
     block_reduce<OpSum, double, kS>(s, red);
-    double f[1] = {0.0};
-    for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x)
-        f[0] = fmax(f[0], fmax(part_r[b * kQ + kQ - 1], part_c[b * kQ + kQ - 1]));
-    block_reduce<OpMax, double, 1>(f, red);
+    // maxima: NaN flag, relative and absolute row violation, dual sign violation
+    double f[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < kCheckBlocks; b += blockDim.x) {
+        const double* r = part_r + b * kQ + kNS;
+        const double* c = part_c + b * kQ + kNS;
+        f[0] = fmax(f[0], fmax(r[0], c[0]));
+        f[1] = fmax(f[1], r[1]);
+        f[2] = fmax(f[2], r[2]);
+        f[3] = fmax(f[3], fmax(r[3], c[3]));
+    }
+    block_reduce<OpMax, double, 4>(f, red);
     if (threadIdx.x != 0) return;
     const double rp_o2 = s[0], rp_s2 = s[1], dobj_r = s[2], dy2 = s[3], fy2 = s[4];
-    const double rd_o2 = s[6], rd_s2 = s[7], pobj_s = s[8], dobj_c = s[9], dx2 = s[10], fx2 = s[11];
+    const double rd_o2 = s[kNS], rd_s2 = s[kNS + 1], pobj_s = s[kNS + 2], dobj_c = s[kNS + 3], dx2 = s[kNS + 4],
+                 fx2 = s[kNS + 5];
     st->total += cp.len;
     st->phase_iters[cp.phase] += cp.len;
     st->restart_flag = 0;
@@ -174,7 +201,12 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
     const double rel = fmax(rel_p, fmax(rel_d, rel_gap));
     st->rel_p = rel_p; st->rel_d = rel_d; st->rel_gap = rel_gap; st->rel_kkt = rel;
     st->pobj = pobj; st->dobj = dobj;
-    if (rel <= cp.tol) {
+    st->viol_p_rel = f[1];
+    st->viol_p_abs = f[2];
+    st->viol_d_abs = f[3];
+    // optimal: relative KKT within tolerance and, when asked, the status guard's maxima too
+    const bool guard_ok = cp.max_violation <= 0.0 || (f[1] <= cp.max_violation && f[3] <= cp.max_violation);
+    if (rel <= cp.tol && guard_ok) {
         st->stop = 1;
         st->status = kStatusOptimal;
         st->stop_iter = st->total;
@@ -852,6 +884,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.pw_smoothing = o.primal_weight_smoothing;
     cp.mixed = mixed ? 1 : 0;
     cp.metric = o.restart_metric == 1 ? 1 : 0;
+    cp.max_violation = o.max_violation;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
     const int64_t max_iter = o.iteration_limit;
 
@@ -989,8 +1022,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     r->objective_value = objective;
     r->dual_objective = is_max ? -hs->dobj : hs->dobj;
     r->restart_count = hs->restart_count;
-    r->primal_residual = hs->rel_p;
-    r->dual_residual = hs->rel_d;
+    r->primal_residual = hs->viol_p_abs;   // max-abs residuals, as PdhgDiagnostics reports them
+    r->dual_residual = hs->viol_d_abs;
     r->duality_gap = hs->rel_gap;
     r->spectral_norm_estimate = spectral_norm;
     r->tau = hs->tau;

@@ -15,6 +15,7 @@ struct HState {
     double kkt_start, kkt_prev;
     double rel_p, rel_d, rel_gap, rel_kkt, pobj, dobj;
     double bnorm, cnorm, offset_min;
+    double viol_p_rel, viol_p_abs, viol_d_abs;   // status-guard maxima of the last check
     double hist[kHist];
     long long k_base;
     long long total;

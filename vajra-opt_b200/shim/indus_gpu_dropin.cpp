@@ -13,8 +13,10 @@
 // "check_frequency".  The backend's own keys:
 //   "vajra_algorithm"  "halpern" (default) or "reference" (the CPU PDHG's semantics, FP64)
 //   "vajra_precision"  "mixed" (default) or "fp64"
-//   "vajra_tolerance"  relative KKT target of "halpern" (default 1e-8, tight enough for the
-//                      engine's 1e-7 primal-feasibility status guard, model.cpp:626-664)
+//   "vajra_tolerance"  relative KKT target of "halpern" (default 1e-8)
+//   "vajra_max_violation"  "halpern" also stops only when the maxima the engine's status guard
+//                      checks (model.cpp:203-374, 626-664) are below this (default 5e-8, half the
+//                      guard's 1e-7), so OPTIMAL results survive the guard
 //   "tolerance", "gap_tolerance" are used by "reference" exactly as the CPU PDHG uses them.
 #include <cmath>
 #include <cstring>
@@ -108,6 +110,9 @@ Solution solve_pdhg_gpu(const Model& model, const Options& options) {
         o.check_frequency = static_cast<int32_t>(options.get_int("check_frequency", 100));
     } else {
         o.tolerance = options.get_double("vajra_tolerance", 1e-8);
+        // the engine re-checks every OPTIMAL result with its status guard (model.cpp:626-664,
+        // 1e-7 absolute or relative); stop only once the guard's maxima are below half of that
+        o.max_violation = options.get_double("vajra_max_violation", 0.5 * tol::kPrimalFeasibility);
         o.check_frequency = static_cast<int32_t>(options.get_int("check_frequency", 64));
     }
     o.iteration_limit = options.iteration_limit;

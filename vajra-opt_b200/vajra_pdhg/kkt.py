@@ -59,3 +59,33 @@ def relative_kkt(lp, x, row_dual) -> dict:
             "primal_objective": pobj, "dual_objective": dobj,
             "max_row_violation": float(np.max(np.abs(rp), initial=0.0)),
             "max_bound_violation": float(max(np.max(cl - x, initial=0.0), np.max(x - cu, initial=0.0)))}
+
+
+def guard_maxima(lp, x, row_dual) -> dict:
+    """The quantities the engine's status guard checks on a returned point
+    (Solution::recompute_quality, src/engine/model.cpp:203-374, LP part; 1e-7 thresholds of
+    include/indus/tolerances.hpp): the largest row violation over 1 + |violated bound| and its
+    absolute size, and the largest reduced-cost / row-dual sign violation (minimisation form,
+    verifier sign convention)."""
+    A = lp.to_scipy_csc()
+    is_max = int(getattr(lp, "sense", 0)) != 0
+    c = -np.asarray(lp.c, float) if is_max else np.asarray(lp.c, float)
+    x = np.asarray(x, float)
+    y = np.asarray(row_dual, float)
+    rl, ru = np.asarray(lp.row_lower, float), np.asarray(lp.row_upper, float)
+    cl, cu = np.asarray(lp.col_lower, float), np.asarray(lp.col_upper, float)
+    ax = A @ x
+    below = np.maximum(rl - ax, 0.0)
+    above = np.maximum(ax - ru, 0.0)
+    den_b = 1.0 + np.where(rl > -1e19, np.abs(rl), 1.0)
+    den_a = 1.0 + np.where(ru < 1e19, np.abs(ru), 1.0)
+    p_rel = float(max(np.max(below / den_b, initial=0.0), np.max(above / den_a, initial=0.0)))
+    p_abs = float(max(np.max(below, initial=0.0), np.max(above, initial=0.0)))
+    d = c - A.T @ y
+    t = 1e-7
+    dv = np.maximum(np.where((x < cu - t) & (d < 0), -d, 0.0), np.where((x > cl + t) & (d > 0), d, 0.0))
+    le = (rl <= -1e20) & (ru < 1e20)
+    ge = (rl > -1e20) & (ru >= 1e20)
+    yv = np.maximum(np.where(le & (y > 0), y, 0.0), np.where(ge & (y < 0), -y, 0.0))
+    return {"primal_rel": p_rel, "primal_abs": p_abs,
+            "dual_abs": float(max(np.max(dv, initial=0.0), np.max(yv, initial=0.0)))}
