@@ -158,6 +158,9 @@ typedef struct vajra_opts {
                                    original LP: each row violation over 1 + |its bound|, each
                                    reduced-cost sign violation of a column off its bound, each
                                    row-dual sign violation (0 = relative KKT only)          */
+    double max_abs_violation;   /* HALPERN: > 0 also requires every row violation of the
+                                   original LP to be at most this in absolute terms (the
+                                   reference verifier's check, src/engine/verifier.cpp)      */
 } vajra_opts;
 
 /* Caller-owned result.  Vector pointers may be NULL (not copied).  Sizes: col_value and

@@ -154,7 +154,7 @@ int solve(int argc, char** argv) {
         opts.use_gpu = true;
         opts.enable_presolve = true;
         opts.iteration_limit = 2000000;
-        opts.time_limit = 300.0;
+        opts.time_limit = 60.0;
         opts.set("vajra_precision", std::string(precision));
         indus::Solution sol = indus::solve(model, opts);
         const std::string sol_path = sol_dir + "/" + name + ".sol";

@@ -151,7 +151,8 @@ struct ControlParams {
     int mixed;        // 1 when an FP32 phase hands over to FP64
     int stall_checks; // FP32 stall window in checks (0 = no stall test; at most kHist - 1)
     int metric;       // restart metric: 0 weighted KKT, 1 fixed-point residual
-    double max_violation;   // > 0: also require the guard's maxima below this
+    double max_violation;       // > 0: also require the guard's maxima below this
+    double max_abs_violation;   // > 0: also require every row violation below this (absolute)
 };
 
 constexpr int kS = 2 * kNS;   // sums the control CTA combines (rows, then columns)
@@ -205,7 +206,8 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
     st->viol_p_abs = f[2];
     st->viol_d_abs = f[3];
     // optimal: relative KKT within tolerance and, when asked, the status guard's maxima too
-    const bool guard_ok = cp.max_violation <= 0.0 || (f[1] <= cp.max_violation && f[3] <= cp.max_violation);
+    const bool guard_ok = (cp.max_violation <= 0.0 || (f[1] <= cp.max_violation && f[3] <= cp.max_violation)) &&
+                          (cp.max_abs_violation <= 0.0 || f[2] <= cp.max_abs_violation);
     if (rel <= cp.tol && guard_ok) {
         st->stop = 1;
         st->status = kStatusOptimal;
@@ -568,8 +570,10 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
     auto time_shapes = [&](CsrView& v, auto launch) -> vajra_status {
         if (v.rows <= 0) return VAJRA_OK;
         constexpr int kFinal = 3;
-        int shapes[10] = {0, kRowblock2, 1, 2, 4, 8, 16, 32, kSell, kSellHot};
-        const int kShapes = v.sell_off ? 10 : 8;
+        // (the hot-prefix sliced-ELL shape is not a candidate: it measured 2x slower than plain
+        // sliced ELL on every LP tried; callers can still force it)
+        int shapes[9] = {0, kRowblock2, 1, 2, 4, 8, 16, 32, kSell};
+        const int kShapes = v.sell_off ? 9 : 8;
         auto timed = [&](int g, int launches, float* ms) -> vajra_status {
             CsrView t = v;
             t.group = g;
@@ -580,14 +584,14 @@ vajra_status autotune_iteration(Phase<T>& ph, CsrView& a, CsrView& at, HState* t
             VJ_CUDA(cudaEventElapsedTime(ms, e0, e1));
             return VAJRA_OK;
         };
-        float first[10];
+        float first[9];
         for (int i = 0; i < kShapes; ++i) {
             CsrView t = v;
             t.group = shapes[i];
             launch(t);   // warm
             VJ_TRY(timed(shapes[i], 3, &first[i]));
         }
-        int order[10];
+        int order[9];
         for (int i = 0; i < kShapes; ++i) order[i] = i;
         std::sort(order, order + kShapes, [&](int a, int b) { return first[a] < first[b]; });
         float total[kFinal] = {0.f, 0.f, 0.f};
@@ -885,6 +889,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.mixed = mixed ? 1 : 0;
     cp.metric = o.restart_metric == 1 ? 1 : 0;
     cp.max_violation = o.max_violation;
+    cp.max_abs_violation = o.max_abs_violation;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
     const int64_t max_iter = o.iteration_limit;
 

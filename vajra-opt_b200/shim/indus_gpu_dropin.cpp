@@ -17,6 +17,8 @@
 //   "vajra_max_violation"  "halpern" also stops only when the maxima the engine's status guard
 //                      checks (model.cpp:203-374, 626-664) are below this (default 5e-8, half the
 //                      guard's 1e-7), so OPTIMAL results survive the guard
+//   "vajra_max_abs_violation"  ... and until every row violation is below this in absolute
+//                      terms (default 5e-7, half the verifier's default 1e-6)
 //   "tolerance", "gap_tolerance" are used by "reference" exactly as the CPU PDHG uses them.
 #include <cmath>
 #include <cstring>
@@ -113,6 +115,8 @@ Solution solve_pdhg_gpu(const Model& model, const Options& options) {
         // the engine re-checks every OPTIMAL result with its status guard (model.cpp:626-664,
         // 1e-7 absolute or relative); stop only once the guard's maxima are below half of that
         o.max_violation = options.get_double("vajra_max_violation", 0.5 * tol::kPrimalFeasibility);
+        // and the verifier's absolute row check (verify_solution, default tolerance 1e-6)
+        o.max_abs_violation = options.get_double("vajra_max_abs_violation", 5e-7);
         o.check_frequency = static_cast<int32_t>(options.get_int("check_frequency", 64));
     }
     o.iteration_limit = options.iteration_limit;
