@@ -203,8 +203,9 @@ def run_study(args, local=0):
 
 def run_adjoint_study(args):
     """Config 4: 256 LPs of 1000 x 3000; gradients of L_i = (w + c).x_i(K) over K = 2000
-    unrolled iterations (checkpoint every 100), FP32 and FP64 forms, against FP64 central
-    differences along random directions, instance by instance.
+    unrolled iterations (checkpoint every 100) -- mixed (the FP64 map's active sets, FP32
+    reverse pass), FP32 and FP64 forms -- against FP64 central differences along random
+    directions, instance by instance.
 
     The unrolled map is piecewise affine in (c, b): a pair (instance, direction) whose forward
     and backward differences disagree beyond rounding has an active-set change within +-h and
@@ -213,7 +214,7 @@ def run_adjoint_study(args):
     reported as well (rounding of the FP64 losses bounds how small h can go)."""
     import numpy as np
     from vajra_pdhg import workloads as W
-    from vajra_pdhg.autograd import PREC_FP64, PREC_MIXED, unrolled
+    from vajra_pdhg.autograd import PREC_FP32, PREC_FP64, PREC_MIXED, unrolled
     lps = [W.random_planted(1000, 3000, 8, seed=1000 + i) for i in range(256)]
     rng = np.random.default_rng(4)
     N = sum(lp.num_cols for lp in lps)
@@ -221,7 +222,7 @@ def run_adjoint_study(args):
     w = rng.standard_normal(N)
     opts = dict(iterations=2000, checkpoint_every=100)
     timing, grads = {}, {}
-    for name, prec in (("fp32", PREC_MIXED), ("fp64", PREC_FP64)):
+    for name, prec in (("mixed", PREC_MIXED), ("fp32", PREC_FP32), ("fp64", PREC_FP64)):
         unrolled(lps[:4], w[: sum(lp.num_cols for lp in lps[:4])], precision=prec, **opts)   # warm
         t0 = time.perf_counter()
         grads[name] = unrolled(lps, w, precision=prec, **opts)
@@ -246,7 +247,7 @@ def run_adjoint_study(args):
     eps = np.finfo(np.float64).eps
     per_h = {}
     for h, ndir in ((1e-6, 32), (1e-8, 32), (1e-9, 64)):
-        errs = {"fp32": [], "fp64": []}
+        errs = {name: [] for name in grads}
         kinks = 0
         for _ in range(ndir):
             dc = rng.standard_normal(N)
@@ -425,6 +426,50 @@ def reference_cpu(lp, iters):
     return {"per_iter_s": per_iter, "setup_s": r["setup_time_sec"], "wall_s": wall,
             "status": r["status_name"], "primal_residual": r["primal_residual"],
             "dual_residual": r["dual_residual"], "iterations": r["iterations"]}
+
+
+def gather_floor(lp, local):
+    """The iteration kernels' gather floor on this LP: vajra_gather_probe_f32 over the same
+    index streams in the degree-ordered numbering the solver uses (A^T y gathers y by row, A x
+    gathers x by column), CUDA events on the launching stream, mean of 10 launches after 3."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from vajra_pdhg import _capi
+    lib = _capi.lib()
+    dev = torch.device("cuda", local)
+    col_deg = np.diff(lp.col_ptr)
+    row_deg = np.bincount(lp.row_idx, minlength=lp.num_rows)
+
+    def rank(deg):      # new index of each old one: descending entry count, ties in index order
+        r = np.empty(len(deg), np.int32)
+        r[np.argsort(-deg, kind="stable")] = np.arange(len(deg), dtype=np.int32)
+        return r
+
+    A = lp.to_scipy_csc().tocsr()
+    streams = {"primal": (rank(row_deg)[lp.row_idx], lp.num_rows), "dual": (rank(col_deg)[A.indices], lp.num_cols)}
+    out = {}
+    for name, (idx_h, size) in streams.items():
+        idx = torch.from_numpy(np.ascontiguousarray(idx_h, np.int32)).to(dev)
+        x = torch.rand(size, device=dev, dtype=torch.float32)
+        threads = C.c_int32(0)
+        lib.vajra_gather_probe_f32(0, None, None, None, C.byref(threads), None)   # size query
+        part = torch.empty(threads.value, device=dev, dtype=torch.float32)
+        st = torch.cuda.current_stream(dev)
+        args = (idx.numel(), C.c_void_p(idx.data_ptr()), C.c_void_p(x.data_ptr()), C.c_void_p(part.data_ptr()),
+                C.byref(threads), C.c_void_p(st.cuda_stream))
+        for _ in range(3):
+            _capi.check(lib.vajra_gather_probe_f32(*args), "vajra_gather_probe_f32")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(10):
+            lib.vajra_gather_probe_f32(*args)
+        e1.record(st)
+        e1.synchronize()
+        us = 1e3 * e0.elapsed_time(e1) / 10
+        out[name] = {"us": round(us, 2), "gathers_per_ns": round(idx.numel() / (us * 1e3), 1)}
+        del idx, x, part
+    return out
 
 
 def workload_config(args, lp):
@@ -617,6 +662,19 @@ def run(args, world, rank, local, dist):
                 "per_kernel_us_gbs": {("primal" if k.startswith("primal") else "dual"):
                                       [round(v[0], 2), round(v[1] / (v[0] * 1e-6) / 1e9, 1) if v[0] > 0 else None]
                                       for k, v in kern.items()}}
+
+    # The gather floor of the two iteration kernels (their index streams, no value stream or
+    # epilogue): how far the dominant kernel is from the random-gather rate of this GPU.
+    try:
+        gf = gather_floor(lp, local)
+        roofline["gather_floor_us"] = {k: v["us"] for k, v in gf.items()}
+        roofline["gathers_per_ns"] = {k: v["gathers_per_ns"] for k, v in gf.items()}
+        roofline["frac_of_gather_floor"] = {
+            k: round(gf[k]["us"] / kern[n][0], 3) for k, n in (("primal", "primal (A^T y + primal prox/Halpern)"),
+                                                             ("dual", "dual (A x_bar + dual prox/Halpern)"))
+            if kern[n][0] > 0}
+    except Exception as e:   # a measurement aid, never required
+        roofline["gather_floor_us"] = f"failed: {e}"
 
     # ---- CPU baseline (rank 0, N = 1) --------------------------------------------------
     cpu = None

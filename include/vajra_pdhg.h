@@ -390,6 +390,16 @@ vajra_status vajra_pdhg_step_f64(int32_t rows, int32_t cols,
                                  double* x, double* x_bar, double* y, double* w, double* v,
                                  void* stream);
 
+/* Measurement probe, no counterpart in the reference: partial sums of x[idx[k]] for k < count
+ * over a grid of resident CTAs (every SM full), 4 independent gathers in flight per thread --
+ * the random gathers of the dense vector that bound the iteration kernels, without their
+ * matrix value stream and epilogue.  Timing it on the iteration kernels' own index stream gives
+ * the gather floor their durations are compared with.  *threads (in: capacity of partials,
+ * out: the number the launch writes); a capacity below that returns INVALID_ARGUMENT with
+ * *threads set to the size needed (count = 0 with NULL arrays queries it). */
+vajra_status vajra_gather_probe_f32(int64_t count, const int32_t* idx, const float* x, float* partials,
+                                    int32_t* threads, void* stream);
+
 /* FP64 relative KKT (the definition the solver's checks use) of a point (x, y) of an LP whose
  * data the caller already holds on the device: A as CSR and as CSC, c, bounds, the column
  * values x and the row duals y in the verifier's sign convention of the minimisation form.

@@ -774,6 +774,24 @@ k_diag_final(int nb, const double* __restrict__ part, vajra_device_diagnostics* 
     }
 }
 
+// Gather-rate probe: sum of x[idx[k]] over all k, 4 independent gathers in flight per thread,
+// grid-stride over a grid of resident CTAs; one partial per thread.  The iteration kernels'
+// random gathers of the dense vector, without their value stream and epilogue.
+__global__ void __launch_bounds__(kThreads)
+k_gather_sum(int64_t n, const int32_t* __restrict__ idx, const float* __restrict__ x, float* __restrict__ out) {
+    const int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    int64_t k = t;
+    for (; k + 3 * stride < n; k += 4 * stride) {
+        const int i0 = __ldcs(idx + k), i1 = __ldcs(idx + k + stride), i2 = __ldcs(idx + k + 2 * stride),
+                  i3 = __ldcs(idx + k + 3 * stride);
+        a0 += __ldg(x + i0); a1 += __ldg(x + i1); a2 += __ldg(x + i2); a3 += __ldg(x + i3);
+    }
+    for (; k < n; k += stride) a0 += __ldg(x + __ldcs(idx + k));
+    out[t] = (a0 + a1) + (a2 + a3);
+}
+
 CsrView exact_view(int rows, const int64_t* ptr, const int32_t* idx) {
     CsrView v;
     v.rows = rows;
@@ -852,6 +870,18 @@ vajra_status vajra_device_diagnostics_f64(int32_t rows, int32_t cols, const doub
     VJ_CUDA(cudaFreeAsync(part, st));
     VJ_CUDA(le);
     note_launch(2);
+    return VAJRA_OK;
+}
+
+vajra_status vajra_gather_probe_f32(int64_t count, const int32_t* idx, const float* x, float* partials,
+                                    int32_t* threads, void* stream) {
+    if (count < 0 || !threads || (count > 0 && (!idx || !x || !partials))) return VAJRA_ERR_INVALID_ARGUMENT;
+    const int grid = sm_count() * (2048 / kThreads);
+    if (*threads < grid * kThreads) { *threads = grid * kThreads; return VAJRA_ERR_INVALID_ARGUMENT; }
+    *threads = grid * kThreads;
+    k_gather_sum<<<grid, kThreads, 0, VJ_STREAM(stream)>>>(count, idx, x, partials);
+    note_launch(1);
+    VJ_LAUNCH_CHECK();
     return VAJRA_OK;
 }
 

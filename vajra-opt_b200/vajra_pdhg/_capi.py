@@ -116,6 +116,7 @@ SIGNATURES = [
      + [C.c_int32, C.c_double, C.c_void_p, C.c_void_p]),
     ("vajra_scale_lp", C.c_int32, [C.POINTER(VajraLp), C.POINTER(VajraOpts)] + [C.c_void_p] * 8),
     ("vajra_release_cached_memory", C.c_int64, [C.c_int32]),
+    ("vajra_gather_probe_f32", C.c_int32, [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 ]
 
 _lib = None
