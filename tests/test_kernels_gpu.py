@@ -163,3 +163,19 @@ def test_device_diagnostics_many_ctas_match_the_oracle(cuda):
     assert d.primal_residual == o["primal_residual"] and d.dual_residual == o["dual_residual"]
     assert d.numerical_error == o["numerical_error"] == 0
     assert abs(d.objective - o["objective"]) <= 1e-9 * (1 + abs(o["objective"]))
+
+
+def test_gather_probe_sums_the_gathered_entries(cuda):
+    """vajra_gather_probe_f32: its per-thread partials add up to sum_k x[idx[k]]."""
+    rng = np.random.default_rng(21)
+    n, count = 300_000, 5_000_003
+    x = rng.random(n).astype(np.float32)
+    idx = rng.integers(0, n, count).astype(np.int32)
+    threads = C.c_int32(0)
+    lib = _capi.lib()
+    assert lib.vajra_gather_probe_f32(0, None, None, None, C.byref(threads), None) == _capi.ERR_INVALID_ARGUMENT
+    assert threads.value > 0
+    ti, tx, tp = dev(idx), dev(x), dev(np.zeros(threads.value, np.float32))
+    assert lib.vajra_gather_probe_f32(count, p(ti), p(tx), p(tp), C.byref(threads), None) == 0
+    want = float(x[idx].astype(np.float64).sum())
+    assert abs(float(host(tp).astype(np.float64).sum()) - want) <= 1e-5 * want
