@@ -370,3 +370,39 @@ def test_max_violation_criterion_meets_the_status_guard(cuda, prec):
     assert abs(g["primal_residual"] - q["primal_abs"]) <= 1e-9 + 1e-6 * q["primal_abs"]
     plain = V.solve(lp, precision=prec)
     assert g["iterations"] >= plain["iterations"]
+
+
+def test_release_cached_memory_returns_blocks_to_the_driver(cuda):
+    import torch
+    lp = W.random_planted(2000, 5000, 8, seed=1)
+    V.solve(lp, precision=V.PREC_MIXED)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    freed = V.release_cached_memory(0)
+    assert freed > 0
+    assert torch.cuda.mem_get_info()[0] >= free0 + freed // 2
+    assert V.release_cached_memory(0) == 0
+
+
+def test_concurrent_solves_reuse_blocks_safely(cuda):
+    """Solves on two host threads (two handles, two streams) share the block cache: a block one
+    solve releases is handed to the other only after the releasing stream's queued work is
+    done.  Every result equals the same solve run alone (solves are deterministic)."""
+    import threading
+    lps = [W.random_planted(1500, 4000, 6, seed=s) for s in (41, 42)]
+    alone = [V.solve(lp, precision=V.PREC_FP64) for lp in lps]
+    out = [[None, None] for _ in lps]
+
+    def worker(k):
+        for rep in range(2):
+            out[k][rep] = V.solve(lps[k], precision=V.PREC_FP64)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for k in range(2):
+        for rep in range(2):
+            for key in ("x", "y", "d"):
+                np.testing.assert_array_equal(out[k][rep][key], alone[k][key], err_msg=f"{k} {rep} {key}")

@@ -41,9 +41,17 @@ vajra_status cuda_status(cudaError_t e, const char* what, const char* file, int 
 
 // ----- device block cache (common.cuh) -------------------------------------------------
 namespace {
+// A cached block and, when it was released while a solve's stream was current, an event
+// recorded on that stream at release: the block is handed out again only once the event has
+// completed (every kernel queued before the release has finished).  Without an event the
+// release waited for the whole device instead.
+struct CachedBlock {
+    void* p;
+    cudaEvent_t ready;
+};
 struct BlockCache {
     std::mutex mu;
-    std::map<std::pair<int, size_t>, std::vector<void*>> free_blocks;
+    std::map<std::pair<int, size_t>, std::vector<CachedBlock>> free_blocks;
     size_t cached_bytes = 0;
 };
 BlockCache& block_cache() {
@@ -58,7 +66,19 @@ size_t size_class(size_t bytes) {
     while (c < bytes) c <<= 1;
     return c;
 }
+thread_local cudaStream_t g_release_stream = nullptr;
+thread_local int g_release_device = -1;
 }  // namespace
+
+ReleaseStreamScope::ReleaseStreamScope(cudaStream_t st, int device)
+    : prev_stream_(g_release_stream), prev_device_(g_release_device) {
+    g_release_stream = st;
+    g_release_device = device;
+}
+ReleaseStreamScope::~ReleaseStreamScope() {
+    g_release_stream = prev_stream_;
+    g_release_device = prev_device_;
+}
 
 // 16 GiB unless VAJRA_BLOCK_CACHE_MB says otherwise (0 keeps no blocks: every release frees).
 size_t block_cache_limit() {
@@ -84,8 +104,9 @@ size_t release_cached_blocks(int device) {
     for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
         if (device >= 0 && it->first.first != device) { ++it; continue; }
         cudaSetDevice(it->first.first);
-        for (void* p : it->second) {
-            cudaFree(p);
+        for (const CachedBlock& b : it->second) {
+            if (b.ready) { cudaEventSynchronize(b.ready); cudaEventDestroy(b.ready); }
+            cudaFree(b.p);
             freed += it->first.second;
         }
         c.cached_bytes -= it->first.second * it->second.size();
@@ -101,16 +122,25 @@ cudaError_t cached_alloc(void** p, size_t bytes, int* device) {
     if (e != cudaSuccess) return e;
     *device = dev;
     const size_t cls = size_class(bytes);
+    CachedBlock b{nullptr, nullptr};
     {
         BlockCache& c = block_cache();
         std::lock_guard<std::mutex> lock(c.mu);
         auto it = c.free_blocks.find({dev, cls});
         if (it != c.free_blocks.end() && !it->second.empty()) {
-            *p = it->second.back();
+            b = it->second.back();
             it->second.pop_back();
             c.cached_bytes -= cls;
-            return cudaSuccess;
         }
+    }
+    if (b.p) {
+        if (b.ready) {   // usually complete already; otherwise wait for the releasing stream
+            cudaError_t w = cudaEventSynchronize(b.ready);
+            cudaEventDestroy(b.ready);
+            if (w != cudaSuccess) { cudaFree(b.p); return w; }
+        }
+        *p = b.p;
+        return cudaSuccess;
     }
     return cudaMalloc(p, cls);
 }
@@ -120,19 +150,36 @@ void cached_release(void* p, size_t bytes, int device) {
     int cur = 0;
     if (cudaGetDevice(&cur) != cudaSuccess) return;
     if (cur != device) cudaSetDevice(device);
-    // Nothing still queued on the device may touch the block once it is handed out again.
-    const bool idle = cudaDeviceSynchronize() == cudaSuccess;
+    // Nothing still queued on the device may touch the block once it is handed out again:
+    // an event on the releasing solve's stream (all of a solve's kernels use it), else the
+    // whole device.  Not inside a stream capture, where neither works: the block is freed.
+    cudaEvent_t ready = nullptr;
+    bool usable = false;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (g_release_stream && g_release_device == device &&
+        cudaStreamIsCapturing(g_release_stream, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone &&
+        cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) == cudaSuccess) {
+        usable = cudaEventRecord(ready, g_release_stream) == cudaSuccess;
+        if (!usable) { cudaEventDestroy(ready); ready = nullptr; }
+    }
+    if (!usable) {
+        cudaGetLastError();
+        usable = cudaDeviceSynchronize() == cudaSuccess;
+    }
     bool kept = false;
-    if (idle) {
+    if (usable) {
         BlockCache& c = block_cache();
         std::lock_guard<std::mutex> lock(c.mu);
         if (c.cached_bytes + cls <= block_cache_limit()) {
-            c.free_blocks[{device, cls}].push_back(p);
+            c.free_blocks[{device, cls}].push_back(CachedBlock{p, ready});
             c.cached_bytes += cls;
             kept = true;
         }
     }
-    if (!kept) cudaFree(p);
+    if (!kept) {
+        if (ready) cudaEventDestroy(ready);
+        cudaFree(p);
+    }
     if (cur != device) cudaSetDevice(cur);
 }
 
@@ -394,6 +441,7 @@ vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra
     if (cudaSetDevice(o.device) != cudaSuccess) return fail(cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__));
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__));
+    ReleaseStreamScope release_scope(h->stream, o.device);
     if (h->m == 0 || h->n == 0 || (h->nnz == 0 && o.algorithm == VAJRA_ALGO_HALPERN)) {
         h->h_c.assign(lp->c, lp->c + h->n);
         h->h_cl.assign(lp->col_lower, lp->col_lower + h->n);
@@ -420,6 +468,7 @@ vajra_status vajra_pdhg_destroy(vajra_pdhg* h) {
     if (!h) return VAJRA_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    ReleaseStreamScope release_scope(h->stream, h->device);
     {
         vajra::DeviceLp empty, empty_ordered;
         vajra::LpOrder empty_order;
@@ -461,6 +510,7 @@ vajra_status vajra_pdhg_run(vajra_pdhg* h, vajra_result* r) {
     r->status_message[0] = '\0';
     vajra_status s = VAJRA_OK;
     const int64_t launches0 = launch_count();
+    ReleaseStreamScope release_scope(h->stream, h->device);
     if (cudaSetDevice(h->device) != cudaSuccess) {
         s = cuda_status(cudaGetLastError(), "cudaSetDevice", __FILE__, __LINE__);
     } else if (solve_trivial(h, r)) {
@@ -597,7 +647,11 @@ vajra_status vajra_pdhg_unrolled(int32_t count, const vajra_lp* lps, const vajra
     cudaStream_t st = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__);
-    vajra_status s = run_unrolled(count, lps, o, weights, loss, x_final, grad_c, grad_row_lower, grad_row_upper, st);
+    vajra_status s;
+    {
+        ReleaseStreamScope release_scope(st, o.device);
+        s = run_unrolled(count, lps, o, weights, loss, x_final, grad_c, grad_row_lower, grad_row_upper, st);
+    }
     if (s != VAJRA_OK) cudaGetLastError();
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
@@ -633,7 +687,11 @@ vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const va
     if (e != cudaSuccess) return cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__);
     const int64_t launches0 = launch_count();
     double dev_time = 0.0;
-    vajra_status s = run_batch(count, lps, o, results, st, &dev_time);
+    vajra_status s;
+    {
+        ReleaseStreamScope release_scope(st, o.device);
+        s = run_batch(count, lps, o, results, st, &dev_time);
+    }
     if (s != VAJRA_OK) {
         for (int k = 0; k < count; ++k) fail_result(&results[k], s);
         cudaGetLastError();

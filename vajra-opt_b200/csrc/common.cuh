@@ -49,7 +49,8 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
 }
 
 // Device blocks go through a process-wide cache keyed by (device, size class): a released
-// block waits for its device to finish all work (the ordering cudaFree gives) and is kept for
+// block is handed out again only after the work queued before its release has finished (the
+// ordering cudaFree gives; see ReleaseStreamScope) and is kept for
 // the next request of its size class on that device, which then needs no driver call.  A
 // solve allocates and releases the same few dozen buffers every run; on shared machines those
 // driver calls were where the occasional multi-second host stalls of a solve showed up.  At
@@ -57,6 +58,19 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
 // their old contents (so does fresh cudaMalloc memory: nothing may assume zeros).
 cudaError_t cached_alloc(void** p, size_t bytes, int* device);
 void cached_release(void* p, size_t bytes, int device);
+// While alive, blocks the calling thread releases on `device` are ordered after the work
+// queued so far on `st` (the stream every kernel of the current solve runs on) by an event,
+// instead of by a device-wide synchronisation.
+class ReleaseStreamScope {
+public:
+    ReleaseStreamScope(cudaStream_t st, int device);
+    ~ReleaseStreamScope();
+    ReleaseStreamScope(const ReleaseStreamScope&) = delete;
+    ReleaseStreamScope& operator=(const ReleaseStreamScope&) = delete;
+private:
+    cudaStream_t prev_stream_;
+    int prev_device_;
+};
 size_t block_cache_limit();
 size_t release_cached_blocks(int device);
 
