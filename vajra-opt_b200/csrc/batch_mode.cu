@@ -42,7 +42,6 @@ struct BatchArrays {      // device struct of arrays, B entries each
 struct BatchCounters {
     int active;
     int pad;
-    long long active_nnz;   // matrix entries of the unfinished instances
 };
 
 __device__ __forceinline__ void instance_weights(const BatchArrays& S, int i) {
@@ -322,31 +321,12 @@ __global__ void k_bcontrol(const double* __restrict__ part, BControl cp, BatchAr
     instance_weights(S, i);
 }
 
-__global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restrict__ done,
-                                                 const int64_t* __restrict__ coff, const int64_t* __restrict__ col_ptr,
-                                                 BatchCounters* out) {
-    __shared__ double red[2 * 32];
-    double v[2] = {0.0, 0.0};   // unfinished instances, their entries (exact in a double below 2^53)
-    for (int i = threadIdx.x; i < count; i += blockDim.x) {
-        if (done[i]) continue;
-        v[0] += 1.0;
-        v[1] += static_cast<double>(col_ptr[coff[i + 1]] - col_ptr[coff[i]]);
-    }
-    block_reduce<OpSum, double, 2>(v, red);
-    if (threadIdx.x == 0) {
-        out->active = static_cast<int>(v[0]);
-        out->active_nnz = static_cast<long long>(v[1]);
-    }
-}
-
-// Lanes per row for the tail of a batched solve, when few small instances are left and an
-// iteration is bound by the latency of each row's chain of gathers rather than by throughput:
-// the power of two nearest the mean row length, 4..32.
-int tail_group(const CsrView& v) {
-    const double mean = v.rows > 0 ? static_cast<double>(v.nnz) / v.rows : 1.0;
-    int g = 4;
-    while (g < 32 && mean > 1.5 * g) g *= 2;
-    return g;
+__global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restrict__ done, BatchCounters* out) {
+    __shared__ double red[32];
+    double v[1] = {0.0};
+    for (int i = threadIdx.x; i < count; i += blockDim.x) v[0] += done[i] ? 0.0 : 1.0;
+    block_reduce<OpSum, double, 1>(v, red);
+    if (threadIdx.x == 0) out->active = static_cast<int>(v[0]);
 }
 
 __global__ void k_brestart(int m, int n, const int* __restrict__ row_inst, const int* __restrict__ col_inst,
@@ -663,29 +643,14 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     BlockList list_a, list_at;
     VJ_TRY(list_a.attach(a_it, row_inst.get(), sms));
     VJ_TRY(list_at.attach(at_it, col_inst.get(), sms));
-    // The tail: once the unfinished instances hold at most 1/kTailShare of the entries, the
-    // shapes tuned for the whole packed matrix leave each remaining row with a long serial
-    // chain of gathers on few CTAs; from then on the chunks run a second graph whose views
-    // give each row more lanes (tail_group).  The switch is one-way and depends only on which
-    // instances are done, so a solve repeats bit for bit.
-    constexpr long long kTailShare = 16;
-    CsrView a_tail = a, at_tail = at;
-    a_tail.group = tail_group(a);
-    at_tail.group = tail_group(at);
-    BlockList tail_a, tail_at;
-    VJ_TRY(tail_a.attach(a_tail, row_inst.get(), sms));
-    VJ_TRY(tail_at.attach(at_tail, col_inst.get(), sms));
 
     DeviceBuffer<BatchCounters> counters;
     VJ_TRY(counters.alloc(1));
     BatchCounters* hc = nullptr;
     VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hc), sizeof(BatchCounters)));
     struct Guard {
-        BatchCounters* h; cudaGraph_t g[2] = {nullptr, nullptr}; cudaGraphExec_t e[2] = {nullptr, nullptr};
-        ~Guard() {
-            for (int k = 0; k < 2; ++k) { if (e[k]) cudaGraphExecDestroy(e[k]); if (g[k]) cudaGraphDestroy(g[k]); }
-            if (h) cudaFreeHost(h);
-        }
+        BatchCounters* h; cudaGraph_t g = nullptr; cudaGraphExec_t e = nullptr;
+        ~Guard() { if (e) cudaGraphExecDestroy(e); if (g) cudaGraphDestroy(g); if (h) cudaFreeHost(h); }
     } guard{hc};
 
     BControl bc{};
@@ -696,26 +661,24 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     bc.pw_smoothing = o.primal_weight_smoothing;
     bc.count = count;
     const double gamma = o.reflection;
-    int64_t graph_kernels[2] = {0, 0};
+    int64_t graph_kernels = 0;
 
-    auto enqueue_chunk = [&](int len, int tail) {
-        const CsrView& a_it_ = tail ? a_tail : a_it;
-        const CsrView& at_it_ = tail ? at_tail : at_it;
-        (tail ? tail_a : list_a).rebuild(S.done, st);
-        (tail ? tail_at : list_at).rebuild(S.done, st);
+    auto enqueue_chunk = [&](int len) {
+        list_a.rebuild(S.done, st);
+        list_at.rebuild(S.done, st);
         for (int kk = 0; kk < len; ++kk) {
             const int wc = kk == len - 1 ? 1 : 0;
             launch_spmv_t<double, double, double>(
-                at_it_, p.csc_val.get(), y.get(),
+                at_it, p.csc_val.get(), y.get(),
                 EpiBPrimal{p.c.get(), p.col_lower.get(), p.col_upper.get(), x0.get(), x.get(), xb.get(), xc.get(),
                            col_inst.get(), S, gamma, kk, wc}, st);
             launch_spmv_t<double, double, double>(
-                a_it_, p.csr_val.get(), xb.get(),
+                a_it, p.csr_val.get(), xb.get(),
                 EpiBDual{p.row_lower.get(), p.row_upper.get(), y0.get(), y.get(), yc.get(), row_inst.get(), S, gamma,
                          kk, wc}, st);
         }
-        launch_spmv_t<double, double, double>(a_it_, p.csr_val.get(), xc.get(), EpiBStore{ax.get(), row_inst.get(), S.done}, st);
-        launch_spmv_t<double, double, double>(at_it_, p.csc_val.get(), yc.get(), EpiBStore{aty.get(), col_inst.get(), S.done}, st);
+        launch_spmv_t<double, double, double>(a_it, p.csr_val.get(), xc.get(), EpiBStore{ax.get(), row_inst.get(), S.done}, st);
+        launch_spmv_t<double, double, double>(at_it, p.csc_val.get(), yc.get(), EpiBStore{aty.get(), col_inst.get(), S.done}, st);
         k_bkkt<<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), ax.get(), aty.get(), xc.get(), yc.get(),
                                            p.row_lower.get(), p.row_upper.get(), lp.row_lower.get(), lp.row_upper.get(),
                                            p.row_scale.get(), p.c.get(), lp.col_lower.get(), lp.col_upper.get(),
@@ -725,39 +688,36 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
         k_bcontrol<<<(count + 127) / 128, 128, 0, st>>>(part.get(), c2, S);
         k_brestart<<<grid_for(mx), kThreads, 0, st>>>(m, n, row_inst.get(), col_inst.get(), xc.get(), yc.get(), x.get(),
                                                       x0.get(), y.get(), y0.get(), x_last.get(), y_last.get(), S);
-        k_bcount<<<1, 1024, 0, st>>>(count, S.done, d_coff.get(), lp.col_ptr.get(), counters.get());
+        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get());
         note_launch(4);
     };
 
     const int64_t max_iter = o.iteration_limit;
     int64_t launched = 0;
     bool time_out = false;
-    int tail = 0;
-    const long long total_nnz = static_cast<long long>(NNZ);
     while (launched < max_iter) {
         const int64_t remaining = max_iter - launched;
         const int len = static_cast<int>(remaining < K ? remaining : K);
         if (len == K) {
-            if (!guard.e[tail]) {
+            if (!guard.e) {
                 const int64_t before = launch_count();
                 VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                enqueue_chunk(len, tail);
-                VJ_CUDA(cudaStreamEndCapture(st, &guard.g[tail]));
-                VJ_CUDA(cudaGraphInstantiate(&guard.e[tail], guard.g[tail], 0));
-                graph_kernels[tail] = launch_count() - before;
+                enqueue_chunk(len);
+                VJ_CUDA(cudaStreamEndCapture(st, &guard.g));
+                VJ_CUDA(cudaGraphInstantiate(&guard.e, guard.g, 0));
+                graph_kernels = launch_count() - before;
                 launch_count() = before;
             }
-            VJ_CUDA(cudaGraphLaunch(guard.e[tail], st));
-            note_launch(graph_kernels[tail]);
+            VJ_CUDA(cudaGraphLaunch(guard.e, st));
+            note_launch(graph_kernels);
         } else {
-            enqueue_chunk(len, tail);
+            enqueue_chunk(len);
             VJ_LAUNCH_CHECK();
         }
         launched += len;
         VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
         VJ_CUDA(cudaStreamSynchronize(st));
         if (hc->active == 0) break;
-        if (!tail && hc->active_nnz * kTailShare <= total_nnz) tail = 1;
         if (seconds_since(t_start) > o.time_limit) { time_out = true; break; }
     }
 
