@@ -151,7 +151,10 @@ typedef struct vajra_opts {
                                    and sums, so every result is bit-identical).  0 auto (MIXED:
                                    on when exact; FP64 form: off), 1 FP64 copy always, 2 the
                                    FP32 copy when exact in either precision                  */
-    int32_t reserved;
+    int32_t handover_mode;      /* MIXED: 0 = the FP64 phase restarts from the FP32 candidate
+                                   (a new Halpern epoch anchored there); 1 = it continues the
+                                   FP32 phase's epoch (iterate, anchor, counter and restart
+                                   references carried over)                                  */
     double max_violation;       /* HALPERN: > 0 also requires, before OPTIMAL, the maxima that
                                    the engine's status guard checks (Solution::recompute_quality,
                                    src/engine/model.cpp:203-374) to be at most this on the

@@ -153,6 +153,7 @@ struct ControlParams {
     int metric;       // restart metric: 0 weighted KKT, 1 fixed-point residual
     double max_violation;       // > 0: also require the guard's maxima below this
     double max_abs_violation;   // > 0: also require every row violation below this (absolute)
+    int handover_mode;          // 0: FP64 phase restarts from the FP32 candidate; 1: continues the epoch
 };
 
 constexpr int kS = 2 * kNS;   // sums the control CTA combines (rows, then columns)
@@ -232,9 +233,13 @@ k_halpern_control(const double* __restrict__ part_r, const double* __restrict__ 
             st->switch_flag = 1;
             st->phase = 1;
             st->gamma_now = cp.gamma64;
-            st->k_base = 0;
-            st->kkt_start = wk;
-            st->kkt_prev = wk;
+            if (cp.handover_mode == 1) {   // the FP64 phase continues the FP32 phase's epoch
+                st->k_base += cp.len;
+            } else {                       // it restarts from the FP32 candidate
+                st->k_base = 0;
+                st->kkt_start = wk;
+                st->kkt_prev = wk;
+            }
             return;
         }
     }
@@ -272,6 +277,18 @@ __global__ void k_halpern_restart(int m, int n, const T* __restrict__ xc, const 
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { const T v = xc[i]; x[i] = v; x0[i] = v; x_last[i] = static_cast<double>(v); }
     if (i < m) { const T v = yc[i]; y[i] = v; y0[i] = v; y_last[i] = static_cast<double>(v); }
+}
+
+// FP32 -> FP64 hand-over that continues the FP32 phase's Halpern epoch: its iterate, anchor
+// and candidate carried over as they are.
+__global__ void k_handover_keep(int m, int n, const float* __restrict__ x32, const float* __restrict__ x032,
+                                const float* __restrict__ xc32, const float* __restrict__ y32,
+                                const float* __restrict__ y032, const float* __restrict__ yc32, double* __restrict__ x,
+                                double* __restrict__ x0, double* __restrict__ xc, double* __restrict__ y,
+                                double* __restrict__ y0, double* __restrict__ yc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { x[i] = x32[i]; x0[i] = x032[i]; xc[i] = xc32[i]; }
+    if (i < m) { y[i] = y32[i]; y0[i] = y032[i]; yc[i] = yc32[i]; }
 }
 
 // FP32 -> FP64 hand-over: the FP32 candidate becomes the FP64 iterate and anchor.
@@ -890,6 +907,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.metric = o.restart_metric == 1 ? 1 : 0;
     cp.max_violation = o.max_violation;
     cp.max_abs_violation = o.max_abs_violation;
+    cp.handover_mode = o.handover_mode == 1 ? 1 : 0;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
     const int64_t max_iter = o.iteration_limit;
 
@@ -945,8 +963,15 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         }
         if (hs->stop) break;
         if (hs->phase != cur_phase) {
-            k_handover<<<grid_for(mx), kThreads, 0, st>>>(m, n, p32.xc.get(), p32.yc.get(), p64.x.get(), p64.x0.get(),
-                                                          p64.xc.get(), p64.y.get(), p64.y0.get(), p64.yc.get());
+            if (o.handover_mode == 1)
+                k_handover_keep<<<grid_for(mx), kThreads, 0, st>>>(m, n, p32.x.get(), p32.x0.get(), p32.xc.get(),
+                                                                   p32.y.get(), p32.y0.get(), p32.yc.get(), p64.x.get(),
+                                                                   p64.x0.get(), p64.xc.get(), p64.y.get(), p64.y0.get(),
+                                                                   p64.yc.get());
+            else
+                k_handover<<<grid_for(mx), kThreads, 0, st>>>(m, n, p32.xc.get(), p32.yc.get(), p64.x.get(),
+                                                              p64.x0.get(), p64.xc.get(), p64.y.get(), p64.y0.get(),
+                                                              p64.yc.get());
             VJ_LAUNCH_CHECK();
             note_launch(1);
             cur_phase = hs->phase;

@@ -44,7 +44,7 @@ class VajraOpts(C.Structure):
                 ("step_safety", C.c_double), ("restart_metric", C.c_int32),
                 ("spmv_shape_a", C.c_int32), ("spmv_shape_at", C.c_int32),
                 ("mixed_reflection", C.c_double), ("degree_order", C.c_int32), ("pow2_scaling", C.c_int32),
-                ("fp64_value_storage", C.c_int32), ("reserved", C.c_int32), ("max_violation", C.c_double),
+                ("fp64_value_storage", C.c_int32), ("handover_mode", C.c_int32), ("max_violation", C.c_double),
                 ("max_abs_violation", C.c_double)]
 
 
