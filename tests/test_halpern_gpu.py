@@ -406,3 +406,12 @@ def test_concurrent_solves_reuse_blocks_safely(cuda):
         for rep in range(2):
             for key in ("x", "y", "d"):
                 np.testing.assert_array_equal(out[k][rep][key], alone[k][key], err_msg=f"{k} {rep} {key}")
+
+
+def test_mixed_handover_continuing_the_fp32_epoch_reaches_the_optimum(cuda):
+    """handover_mode = 1: the FP64 phase takes over the FP32 phase's iterate, anchor, Halpern
+    counter and restart references instead of restarting from the FP32 candidate."""
+    lp = W.random_planted(2000, 5000, 8, seed=24)
+    g = V.solve(lp, precision=V.PREC_MIXED, handover_mode=1, mixed_switch_tolerance=1e-4)
+    assert g["fp32_iterations"] > 0 and g["fp64_iterations"] > 0
+    check_solution(lp, g, obj=lp.planted_objective)
