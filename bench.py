@@ -120,7 +120,7 @@ def batch_line(args, world=1, rank=0, dist=None, sequential=True):
     if rank != 0:
         return None
     iters = [s["iterations"] for s in summaries]
-    line = {"metric": "batched solves/s vs sequential plain FP64 solves (rel KKT 1e-6 each)",
+    line = {"metric": "batched (mixed precision) solves/s vs sequential plain FP64 solves (rel KKT 1e-6 each)",
             "value": len(lps) / batch_wall, "unit": "solves/s", "higher_is_better": True, "n_gpus": world,
             "scaling": "strong",
             "batch": {"count": len(lps), "nnz": nnz, "wall_s": batch_wall, "device_s": batch_dev, "optimal": ok,
@@ -133,6 +133,12 @@ def batch_line(args, world=1, rank=0, dist=None, sequential=True):
                                    f"nnz per column U{{4..12}}, planted optima, seed 3",
                        "parallelism": f"instances sharded by nnz over {world} rank(s)"}}
     if world == 1 and sequential:
+        # the same batch with the FP64 pass alone (the plain form), for the precision split's share
+        t0 = time.perf_counter()
+        rb = V.solve_batch(lps, precision=V.PREC_FP64)
+        line["batch_fp64"] = {"wall_s": time.perf_counter() - t0, "device_s": rb[0]["device_time_sec"],
+                              "optimal": sum(r["status_name"] == "OPTIMAL" for r in rb),
+                              "max_iterations": max(r["iterations"] for r in rb)}
         nseq = len(lps) if args.batch_sequential < 0 else min(args.batch_sequential, len(lps))
         V.solve(lps[0], precision=V.PREC_FP64)
         seq_times, seq_ok = [], 0

@@ -272,9 +272,12 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
  * (pdhg_cuda.cu:187-227 upload once): create uploads the LP to the device; run does the
  * device set-up and the solve from the resident copy; destroy frees it. */
 vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra_pdhg** handle);
-/* Batched form: `count` independent LPs solved together (VAJRA_ALGO_HALPERN, FP64), packed
+/* Batched form: `count` independent LPs solved together (VAJRA_ALGO_HALPERN), packed
  * block-diagonally into one device problem with per-instance step sizes, primal weights,
- * restarts and termination.  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
+ * restarts and termination.  VAJRA_PREC_MIXED runs an FP32 pass first (FP32 values, iterates
+ * and sums, FP64 checks), in which each instance either reaches the tolerance or -- at
+ * mixed_switch_tolerance or on a stall -- hands over to an FP64 pass that restarts it from its
+ * FP32 candidate; VAJRA_PREC_FP64 runs the FP64 pass alone.  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
  * the reference's benchmark Suite 2 issues them (apps/benchmark_runner.cpp:936-944).
  * results[i] receives instance i; every result's device_time_sec is the whole batch's. */
 vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const vajra_opts* opts,

@@ -64,3 +64,29 @@ def test_batch_iteration_limit(cuda):
     for r in res:
         assert r["status_name"] in ("ITERATION_LIMIT", "OPTIMAL")
         assert r["iterations"] <= 64
+
+
+def test_batch_mixed_and_fp64_passes(cuda):
+    """Mixed precision: every instance runs an FP32 pass first and finishes there or in the FP64
+    pass after its hand-over; the plain form runs FP64 only.  Both reach the planted optima."""
+    lps = small_batch(12, seed=9)
+    mixed = V.solve_batch(lps, precision=V.PREC_MIXED)
+    plain = V.solve_batch(lps, precision=V.PREC_FP64)
+    assert any(r["fp32_iterations"] > 0 for r in mixed)
+    assert all(r["fp32_iterations"] == 0 for r in plain)
+    for lp, a, b in zip(lps, mixed, plain):
+        for r in (a, b):
+            assert r["status_name"] == "OPTIMAL", r["status_message"]
+            assert r["fp32_iterations"] + r["fp64_iterations"] == r["iterations"]
+            assert relative_kkt(lp, r["x"], r["y"])["rel_kkt"] <= 1.05e-6
+            assert abs(r["objective_value"] - lp.planted_objective) <= 1e-5 * (1 + abs(lp.planted_objective))
+
+
+def test_batch_mixed_iteration_limit_inside_the_fp32_pass(cuda):
+    """A limit reached in the FP32 pass reports the FP32 candidates, widened, as limit results."""
+    lps = small_batch(4, seed=10)
+    res = V.solve_batch(lps, precision=V.PREC_MIXED, iteration_limit=128)
+    for lp, r in zip(lps, res):
+        assert r["status_name"] in ("ITERATION_LIMIT", "OPTIMAL")
+        assert r["iterations"] <= 128 and r["fp64_iterations"] == 0
+        assert np.all(np.isfinite(r["x"])) and np.all(np.isfinite(r["y"]))

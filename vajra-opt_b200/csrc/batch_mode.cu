@@ -1,5 +1,8 @@
 // Batched restarted Halpern PDHG: many independent LPs of uneven sizes packed
-// block-diagonally into one device problem (FP64 iterates, the plain form).
+// block-diagonally into one device problem.  In mixed precision an FP32 pass (FP32 values,
+// iterates and sums; FP64 checks) comes first, and each instance either finishes there or
+// hands over to the FP64 pass, which restarts it from its FP32 candidate -- the single-LP
+// solver's precision split, decided per instance.
 //
 // The packed matrix diag(A_1, ..., A_B) is one CSC / CSR, so each iteration is still two
 // fused SpMV launches over all instances.  Every instance keeps its own step sizes, primal
@@ -33,11 +36,18 @@ struct BatchArrays {      // device struct of arrays, B entries each
     double* rel_p; double* rel_d; double* rel_gap; double* rel_kkt; double* pobj; double* dobj;
     double* bnorm; double* cnorm; double* offset_min; double* lambda;
     double* inv_sigma;    // 1 / sigma
+    double* gamma;        // reflection of the instance's current phase
     double* hw;           // Halpern weights of the current chunk, 2 hw_len per instance:
     int hw_len;           // hw[i 2 hw_len + 2 kk] = (k+1)/(k+2), [.. + 1] = 1/(k+2), k = k_base + kk
+    double* hist;         // FP32 pass: the last kBHist relative KKT values per instance (stall test)
     long long* k_base; long long* total;
-    int* done; int* status; int* restart_count; int* restart_flag;
+    long long* total32;   // iterations the instance spent in the FP32 pass
+    int* done; int* status; int* restart_count; int* restart_flag; int* hist_n;
 };
+
+constexpr int kBHist = 32;
+// Status of an instance that left the FP32 pass for the FP64 one (internal, never reported).
+constexpr int kBHandover = 100;
 
 struct BatchCounters {
     int active;
@@ -61,15 +71,15 @@ __device__ __forceinline__ bool any_active(const int* done, const int* inst, int
     return false;
 }
 
+template <typename T>
 struct EpiBPrimal {
-    const double* c; const double* cl; const double* cu; const double* x0;
-    double* x; double* xb; double* xc;
+    const T* c; const T* cl; const T* cu; const T* x0;
+    T* x; T* xb; T* xc;
     const int* col_inst;
     BatchArrays S;
-    double gamma;
     int kk, write_cand;
     // two-phase (spmv.cuh): the instance lookups and vector loads go out before the SpMV's
-    struct Pre { double w1, w0, tau, xo, c, cl, cu, x0; int done; };
+    struct Pre { T w1, w0, tau, g, xo, c, cl, cu, x0; int done; };
     __device__ bool active() const { return true; }
     __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, col_inst, r0, r1); }
     __device__ Pre pre(int j) const {
@@ -77,9 +87,10 @@ struct EpiBPrimal {
         Pre p;
         p.done = S.done[i];
         const double* w = S.hw + static_cast<size_t>(i) * 2 * S.hw_len + 2 * kk;
-        p.w1 = w[0];
-        p.w0 = w[1];
-        p.tau = S.tau[i];
+        p.w1 = static_cast<T>(w[0]);
+        p.w0 = static_cast<T>(w[1]);
+        p.tau = static_cast<T>(S.tau[i]);
+        p.g = static_cast<T>(S.gamma[i]);
         p.xo = x[j];
         p.c = __ldg(c + j);
         p.cl = __ldg(cl + j);
@@ -87,25 +98,27 @@ struct EpiBPrimal {
         p.x0 = __ldg(x0 + j);
         return p;
     }
-    __device__ void operator()(int j, double v, const Pre& p) const {
+    template <typename Acc>
+    __device__ void operator()(int j, Acc v, const Pre& p) const {
         if (p.done) return;
-        double xp = p.xo - p.tau * (p.c + v);
+        T xp = p.xo - p.tau * (p.c + static_cast<T>(v));
         xp = xp < p.cl ? p.cl : (xp > p.cu ? p.cu : xp);
         xb[j] = xp + xp - p.xo;
-        x[j] = p.w1 * ((1.0 + gamma) * xp - gamma * p.xo) + p.w0 * p.x0;
+        x[j] = p.w1 * ((T(1) + p.g) * xp - p.g * p.xo) + p.w0 * p.x0;
         if (write_cand) xc[j] = xp;
     }
-    __device__ void operator()(int j, double v) const { (*this)(j, v, pre(j)); }
+    template <typename Acc>
+    __device__ void operator()(int j, Acc v) const { (*this)(j, v, pre(j)); }
 };
 
+template <typename T>
 struct EpiBDual {
-    const double* rl; const double* ru; const double* y0;
-    double* y; double* yc;
+    const T* rl; const T* ru; const T* y0;
+    T* y; T* yc;
     const int* row_inst;
     BatchArrays S;
-    double gamma;
     int kk, write_cand;
-    struct Pre { double w1, w0, sigma, inv_sigma, yo, rl, ru, y0; int done; };
+    struct Pre { T w1, w0, sigma, inv_sigma, g, yo, rl, ru, y0; int done; };
     __device__ bool active() const { return true; }
     __device__ bool skip_rows(int r0, int r1) const { return !any_active(S.done, row_inst, r0, r1); }
     __device__ Pre pre(int r) const {
@@ -113,27 +126,30 @@ struct EpiBDual {
         Pre p;
         p.done = S.done[i];
         const double* w = S.hw + static_cast<size_t>(i) * 2 * S.hw_len + 2 * kk;
-        p.w1 = w[0];
-        p.w0 = w[1];
-        p.sigma = S.sigma[i];
-        p.inv_sigma = S.inv_sigma[i];
+        p.w1 = static_cast<T>(w[0]);
+        p.w0 = static_cast<T>(w[1]);
+        p.sigma = static_cast<T>(S.sigma[i]);
+        p.inv_sigma = static_cast<T>(S.inv_sigma[i]);
+        p.g = static_cast<T>(S.gamma[i]);
         p.yo = y[r];
         p.rl = __ldg(rl + r);
         p.ru = __ldg(ru + r);
         p.y0 = __ldg(y0 + r);
         return p;
     }
-    __device__ void operator()(int r, double w, const Pre& p) const {
+    template <typename Acc>
+    __device__ void operator()(int r, Acc w, const Pre& p) const {
         if (p.done) return;
-        const double sg = p.sigma;
-        const double yh = p.yo + sg * w;
-        double q = yh * p.inv_sigma;
+        const T sg = p.sigma;
+        const T yh = p.yo + sg * static_cast<T>(w);
+        T q = yh * p.inv_sigma;
         q = q < p.rl ? p.rl : (q > p.ru ? p.ru : q);
-        const double yp = yh - sg * q;
-        y[r] = p.w1 * ((1.0 + gamma) * yp - gamma * p.yo) + p.w0 * p.y0;
+        const T yp = yh - sg * q;
+        y[r] = p.w1 * ((T(1) + p.g) * yp - p.g * p.yo) + p.w0 * p.y0;
         if (write_cand) yc[r] = yp;
     }
-    __device__ void operator()(int r, double w) const { (*this)(r, w, pre(r)); }
+    template <typename Acc>
+    __device__ void operator()(int r, Acc w) const { (*this)(r, w, pre(r)); }
 };
 
 struct EpiBStore {
@@ -214,9 +230,10 @@ __device__ __forceinline__ bool lo_fin(double l) { return l > -1e20; }
 __device__ __forceinline__ bool up_fin(double u) { return u < 1e20; }
 
 // One CTA per instance: the same KKT terms as the single-LP row / column passes.
+template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_bkkt(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const double* __restrict__ ax,
-       const double* __restrict__ aty, const double* __restrict__ xc, const double* __restrict__ yc,
+       const double* __restrict__ aty, const T* __restrict__ xc, const T* __restrict__ yc,
        const double* __restrict__ rl_s, const double* __restrict__ ru_s, const double* __restrict__ rl_o,
        const double* __restrict__ ru_o, const double* __restrict__ rs, const double* __restrict__ c_s,
        const double* __restrict__ cl_o, const double* __restrict__ cu_o, const double* __restrict__ cs,
@@ -228,7 +245,7 @@ k_bkkt(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const
     double v[kBQ] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // 0 rp_o^2, 1 rp_s^2, 2 dobj rows, 3 dy^2, 4 rd_o^2, 5 rd_s^2, 6 pobj, 7 dobj cols, 8 dx^2, 9 nan
     for (int64_t i = roff[inst] + threadIdx.x; i < roff[inst + 1]; i += blockDim.x) {
-        const double a = ax[i], ys = yc[i];
+        const double a = ax[i], ys = static_cast<double>(yc[i]);
         if (!isfinite(a) || !isfinite(ys)) v[9] = 1.0;
         const double ps = a - fmin(fmax(a, rl_s[i]), ru_s[i]);
         const double ao = a / rs[i];
@@ -241,7 +258,7 @@ k_bkkt(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const
         v[0] += po * po; v[1] += ps * ps; v[2] += dt; v[3] += dy * dy;
     }
     for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x) {
-        const double at = aty[j], xs = xc[j];
+        const double at = aty[j], xs = static_cast<double>(xc[j]);
         if (!isfinite(at) || !isfinite(xs)) v[9] = 1.0;
         const bool lf = lo_fin(cl_o[j]), uf = up_fin(cu_o[j]);
         const double r_s = c_s[j] + at, r_o = r_s / cs[j];
@@ -266,6 +283,12 @@ k_bkkt(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const
 struct BControl {
     double tol, beta_sufficient, beta_necessary, beta_artificial, pw_smoothing;
     int len, count;
+    // FP32 pass of a mixed batch (same rules as the single-LP FP32 phase, per instance):
+    int pass32;            // 1 while the FP32 pass runs
+    double switch_tol;     // hand over to FP64 at or below this relative KKT ...
+    int stall_checks;      // ... or after this many checks with < 2 % gain (0 = never)
+    double early_tol;      // below this the FP32 pass reflects with gamma32
+    double gamma32;
 };
 
 // One thread per instance: the single-LP control rules (halpern_mode.cu) per instance.
@@ -292,6 +315,20 @@ __global__ void k_bcontrol(const double* __restrict__ part, BControl cp, BatchAr
         S.done[i] = 1;
         S.status[i] = 1;
         return;
+    }
+    if (cp.pass32) {
+        const int hn = S.hist_n[i];
+        double* hist = S.hist + static_cast<size_t>(i) * kBHist;
+        const int w = cp.stall_checks;
+        const bool stalled = w > 0 && hn >= w && rel > 0.98 * hist[(hn - w) % kBHist];
+        hist[hn % kBHist] = rel;
+        S.hist_n[i] = hn + 1;
+        if (rel <= cp.early_tol) S.gamma[i] = cp.gamma32;
+        if (rel <= cp.switch_tol || stalled) {   // leaves the FP32 pass; the FP64 pass takes it over
+            S.done[i] = 1;
+            S.status[i] = kBHandover;
+            return;
+        }
     }
     const double omega = S.omega[i];
     const double wk = sqrt(omega * s[1] + s[5] / omega + gap * gap);
@@ -329,13 +366,61 @@ __global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restric
     if (threadIdx.x == 0) out->active = static_cast<int>(v[0]);
 }
 
+template <typename T>
 __global__ void k_brestart(int m, int n, const int* __restrict__ row_inst, const int* __restrict__ col_inst,
-                           const double* __restrict__ xc, const double* __restrict__ yc, double* __restrict__ x,
-                           double* __restrict__ x0, double* __restrict__ y, double* __restrict__ y0,
+                           const T* __restrict__ xc, const T* __restrict__ yc, T* __restrict__ x,
+                           T* __restrict__ x0, T* __restrict__ y, T* __restrict__ y0,
                            double* __restrict__ x_last, double* __restrict__ y_last, BatchArrays S) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n && S.restart_flag[col_inst[t]]) { const double v = xc[t]; x[t] = v; x0[t] = v; x_last[t] = v; }
-    if (t < m && S.restart_flag[row_inst[t]]) { const double v = yc[t]; y[t] = v; y0[t] = v; y_last[t] = v; }
+    if (t < n && S.restart_flag[col_inst[t]]) { const T v = xc[t]; x[t] = v; x0[t] = v; x_last[t] = v; }
+    if (t < m && S.restart_flag[row_inst[t]]) { const T v = yc[t]; y[t] = v; y0[t] = v; y_last[t] = v; }
+}
+
+// End of the FP32 pass, vectors: every instance's FP32 candidate becomes its FP64 candidate
+// (the point post-processing reports for instances that finished in FP32 or hit a limit), and
+// an instance that was handed over also starts its FP64 pass there (iterate, anchor and last
+// restart point), as the single-LP hand-over does.
+__global__ void k_bhandover(int m, int n, const int* __restrict__ row_inst, const int* __restrict__ col_inst,
+                            const float* __restrict__ xc32, const float* __restrict__ yc32, double* __restrict__ x,
+                            double* __restrict__ x0, double* __restrict__ xc, double* __restrict__ x_last,
+                            double* __restrict__ y, double* __restrict__ y0, double* __restrict__ yc,
+                            double* __restrict__ y_last, const int* __restrict__ status) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        const double v = xc32[t];
+        xc[t] = v;
+        if (status[col_inst[t]] == kBHandover) { x[t] = v; x0[t] = v; x_last[t] = v; }
+    }
+    if (t < m) {
+        const double v = yc32[t];
+        yc[t] = v;
+        if (status[row_inst[t]] == kBHandover) { y[t] = v; y0[t] = v; y_last[t] = v; }
+    }
+}
+
+// End of the FP32 pass, per-instance state: its iterations are counted as FP32 ones, and a
+// handed-over instance starts a fresh Halpern epoch with the FP64 reflection (primal weight
+// and step sizes carry over).
+__global__ void k_bhandover_state(int count, double gamma64, BatchArrays S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    S.total32[i] = S.total[i];
+    if (S.status[i] != kBHandover) return;
+    S.done[i] = 0;
+    S.status[i] = 0;
+    S.k_base[i] = 0;
+    S.kkt_start[i] = -1.0;
+    S.kkt_prev[i] = -1.0;
+    S.gamma[i] = gamma64;
+    S.restart_flag[i] = 0;
+    instance_weights(S, i);
+}
+
+template <typename To>
+__global__ void k_bconvert(int64_t n, const double* __restrict__ src, To* __restrict__ dst) {
+    for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+         k += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[k] = static_cast<To>(src[k]);
 }
 
 // Per-instance norms (||b||, ||c|| original; ||b||, ||c|| scaled) and initial state.
@@ -343,7 +428,7 @@ __global__ void __launch_bounds__(kThreads)
 k_binit(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const double* __restrict__ rl_o,
         const double* __restrict__ ru_o, const double* __restrict__ c_o, const double* __restrict__ rl_s,
         const double* __restrict__ ru_s, const double* __restrict__ c_s, const int* __restrict__ sense,
-        const double* __restrict__ offsets, double step_safety, BatchArrays S) {
+        const double* __restrict__ offsets, double step_safety, double gamma0, BatchArrays S) {
     const int inst = blockIdx.x;
     __shared__ double red[4 * 32];
     double v[4] = {0, 0, 0, 0};
@@ -373,6 +458,8 @@ k_binit(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, cons
     S.offset_min[inst] = sense[inst] ? -offsets[inst] : offsets[inst];
     S.k_base[inst] = 0; S.total[inst] = 0;
     S.done[inst] = 0; S.status[inst] = 0; S.restart_count[inst] = 0; S.restart_flag[inst] = 0;
+    S.hist_n[inst] = 0; S.total32[inst] = 0;
+    S.gamma[inst] = gamma0;
     S.rel_kkt[inst] = 1e30;
     instance_weights(S, inst);
 }
@@ -548,23 +635,26 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     DeviceBuffer<double> dd;
     DeviceBuffer<long long> dl;
     DeviceBuffer<int> di;
-    VJ_TRY(dd.alloc(17 * static_cast<size_t>(count)));
+    VJ_TRY(dd.alloc(18 * static_cast<size_t>(count)));
     const int K = o.check_frequency > 0 ? o.check_frequency : 64;
-    DeviceBuffer<double> d_hw;
+    DeviceBuffer<double> d_hw, d_hist;
     VJ_TRY(d_hw.alloc(2 * static_cast<size_t>(K) * count));
-    VJ_TRY(dl.alloc(2 * static_cast<size_t>(count)));
-    VJ_TRY(di.alloc(4 * static_cast<size_t>(count)));
+    VJ_TRY(d_hist.alloc(static_cast<size_t>(kBHist) * count));
+    VJ_TRY(dl.alloc(3 * static_cast<size_t>(count)));
+    VJ_TRY(di.alloc(5 * static_cast<size_t>(count)));
     BatchArrays S;
     double** fields[] = {&S.omega, &S.eta, &S.tau, &S.sigma, &S.kkt_start, &S.kkt_prev, &S.rel_p, &S.rel_d,
                          &S.rel_gap, &S.rel_kkt, &S.pobj, &S.dobj, &S.bnorm, &S.cnorm, &S.offset_min, &S.lambda,
-                         &S.inv_sigma};
-    for (int q = 0; q < 17; ++q) *fields[q] = dd.get() + static_cast<size_t>(q) * count;
+                         &S.inv_sigma, &S.gamma};
+    for (int q = 0; q < 18; ++q) *fields[q] = dd.get() + static_cast<size_t>(q) * count;
     S.hw = d_hw.get();
     S.hw_len = K;
-    S.k_base = dl.get(); S.total = dl.get() + count;
+    S.hist = d_hist.get();
+    S.k_base = dl.get(); S.total = dl.get() + count; S.total32 = dl.get() + 2 * count;
     S.done = di.get(); S.status = di.get() + count; S.restart_count = di.get() + 2 * count;
     S.restart_flag = di.get() + 3 * count;
-    VJ_CUDA(cudaMemsetAsync(di.get(), 0, sizeof(int) * 4 * count, st));   // done = 0 for the power iteration
+    S.hist_n = di.get() + 4 * count;
+    VJ_CUDA(cudaMemsetAsync(di.get(), 0, sizeof(int) * 5 * count, st));   // done = 0 for the power iteration
 
     // batched power iteration (fixed 60 rounds)
     {
@@ -586,7 +676,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     const double safety = (o.step_safety > 0.0 && o.step_safety < 1.0) ? o.step_safety : 0.99;
     k_binit<<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), lp.row_lower.get(), lp.row_upper.get(), d_cmin.get(),
                                         p.row_lower.get(), p.row_upper.get(), p.c.get(), d_sense.get(), d_offsets.get(),
-                                        safety, S);
+                                        safety, o.reflection, S);
     note_launch(1);
 
     // iterates
@@ -600,6 +690,27 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
                                                         y_last.get());
     note_launch(1);
     VJ_LAUNCH_CHECK();
+    // Mixed precision: an FP32 pass (FP32 values, iterates and sums, FP64 checks) runs first;
+    // each instance finishes there or hands over to the FP64 pass.
+    const bool mixed = o.precision == VAJRA_PREC_MIXED;
+    DeviceBuffer<float> x32, x0_32, xb32, xc32, y32, y0_32, yc32, c32, cl32, cu32, rl32, ru32;
+    if (mixed) {
+        VJ_TRY(make_f32_values(p, NNZ, st));
+        for (auto* b : {&x32, &x0_32, &xb32, &xc32, &c32, &cl32, &cu32}) VJ_TRY(b->alloc(n));
+        for (auto* b : {&y32, &y0_32, &yc32, &rl32, &ru32}) VJ_TRY(b->alloc(m));
+        const unsigned gn = grid_for(n, kThreads, 148 * 32), gm = grid_for(m, kThreads, 148 * 32);
+        k_bconvert<float><<<gn, kThreads, 0, st>>>(n, p.c.get(), c32.get());
+        k_bconvert<float><<<gn, kThreads, 0, st>>>(n, p.col_lower.get(), cl32.get());
+        k_bconvert<float><<<gn, kThreads, 0, st>>>(n, p.col_upper.get(), cu32.get());
+        k_bconvert<float><<<gm, kThreads, 0, st>>>(m, p.row_lower.get(), rl32.get());
+        k_bconvert<float><<<gm, kThreads, 0, st>>>(m, p.row_upper.get(), ru32.get());
+        for (auto* b : {&x32, &x0_32, &xb32, &xc32})
+            k_bconvert<float><<<gn, kThreads, 0, st>>>(n, x.get(), b->get());
+        for (auto* b : {&y32, &y0_32, &yc32})
+            k_bconvert<float><<<gm, kThreads, 0, st>>>(m, y.get(), b->get());
+        note_launch(12);
+        VJ_LAUNCH_CHECK();
+    }
 
     // autotune the packed SpMVs (store epilogue, no skipping)
     CsrView a = p.a, at = p.at;
@@ -649,8 +760,11 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     BatchCounters* hc = nullptr;
     VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hc), sizeof(BatchCounters)));
     struct Guard {
-        BatchCounters* h; cudaGraph_t g = nullptr; cudaGraphExec_t e = nullptr;
-        ~Guard() { if (e) cudaGraphExecDestroy(e); if (g) cudaGraphDestroy(g); if (h) cudaFreeHost(h); }
+        BatchCounters* h; cudaGraph_t g[2] = {nullptr, nullptr}; cudaGraphExec_t e[2] = {nullptr, nullptr};
+        ~Guard() {
+            for (int k = 0; k < 2; ++k) { if (e[k]) cudaGraphExecDestroy(e[k]); if (g[k]) cudaGraphDestroy(g[k]); }
+            if (h) cudaFreeHost(h);
+        }
     } guard{hc};
 
     BControl bc{};
@@ -660,34 +774,58 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     bc.beta_artificial = o.restart_artificial;
     bc.pw_smoothing = o.primal_weight_smoothing;
     bc.count = count;
-    const double gamma = o.reflection;
-    int64_t graph_kernels = 0;
+    bc.switch_tol = o.mixed_switch_tolerance;
+    bc.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kBHist - 1 ? kBHist - 1 : o.mixed_stall_checks);
+    bc.early_tol = 10.0 * o.mixed_switch_tolerance;   // as the single-LP FP32 phase
+    bc.gamma32 = (o.mixed_reflection > 0.0 && o.mixed_reflection <= 1.0) ? o.mixed_reflection : o.reflection;
+    int64_t graph_kernels[2] = {0, 0};
 
-    auto enqueue_chunk = [&](int len) {
+    // One chunk of a pass in precision T (its iterates, values and bounds in T; the checks read
+    // the FP64 values).  Pass 0 is the FP32 pass, pass 1 the FP64 one.
+    struct PassBuffers {
+        const void* csr; const void* csc;
+        const void* c; const void* cl; const void* cu; const void* rl; const void* ru;
+        void* x; void* x0; void* xb; void* xc; void* y; void* y0; void* yc;
+    };
+    const PassBuffers pb64{p.csr_val.get(), p.csc_val.get(), p.c.get(), p.col_lower.get(), p.col_upper.get(),
+                           p.row_lower.get(), p.row_upper.get(), x.get(), x0.get(), xb.get(), xc.get(), y.get(),
+                           y0.get(), yc.get()};
+    const PassBuffers pb32{p.csr_val32.get(), p.csc_val32.get(), c32.get(), cl32.get(), cu32.get(), rl32.get(),
+                           ru32.get(), x32.get(), x0_32.get(), xb32.get(), xc32.get(), y32.get(), y0_32.get(),
+                           yc32.get()};
+    auto chunk = [&](auto tag, int len) {
+        using T = decltype(tag);
+        const PassBuffers& b = sizeof(T) == 4 ? pb32 : pb64;
+        const T* csr = static_cast<const T*>(b.csr);
+        const T* csc = static_cast<const T*>(b.csc);
+        T* xv = static_cast<T*>(b.x); T* x0v = static_cast<T*>(b.x0); T* xbv = static_cast<T*>(b.xb);
+        T* xcv = static_cast<T*>(b.xc); T* yv = static_cast<T*>(b.y); T* y0v = static_cast<T*>(b.y0);
+        T* ycv = static_cast<T*>(b.yc);
         list_a.rebuild(S.done, st);
         list_at.rebuild(S.done, st);
         for (int kk = 0; kk < len; ++kk) {
             const int wc = kk == len - 1 ? 1 : 0;
-            launch_spmv_t<double, double, double>(
-                at_it, p.csc_val.get(), y.get(),
-                EpiBPrimal{p.c.get(), p.col_lower.get(), p.col_upper.get(), x0.get(), x.get(), xb.get(), xc.get(),
-                           col_inst.get(), S, gamma, kk, wc}, st);
-            launch_spmv_t<double, double, double>(
-                a_it, p.csr_val.get(), xb.get(),
-                EpiBDual{p.row_lower.get(), p.row_upper.get(), y0.get(), y.get(), yc.get(), row_inst.get(), S, gamma,
-                         kk, wc}, st);
+            launch_spmv_t<T, T, T>(at_it, csc, yv,
+                                   EpiBPrimal<T>{static_cast<const T*>(b.c), static_cast<const T*>(b.cl),
+                                                 static_cast<const T*>(b.cu), x0v, xv, xbv, xcv, col_inst.get(), S,
+                                                 kk, wc}, st);
+            launch_spmv_t<T, T, T>(a_it, csr, xbv,
+                                   EpiBDual<T>{static_cast<const T*>(b.rl), static_cast<const T*>(b.ru), y0v, yv, ycv,
+                                               row_inst.get(), S, kk, wc}, st);
         }
-        launch_spmv_t<double, double, double>(a_it, p.csr_val.get(), xc.get(), EpiBStore{ax.get(), row_inst.get(), S.done}, st);
-        launch_spmv_t<double, double, double>(at_it, p.csc_val.get(), yc.get(), EpiBStore{aty.get(), col_inst.get(), S.done}, st);
-        k_bkkt<<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), ax.get(), aty.get(), xc.get(), yc.get(),
-                                           p.row_lower.get(), p.row_upper.get(), lp.row_lower.get(), lp.row_upper.get(),
-                                           p.row_scale.get(), p.c.get(), lp.col_lower.get(), lp.col_upper.get(),
-                                           p.col_scale.get(), x_last.get(), y_last.get(), part.get(), S);
+        launch_spmv_t<double, T, double>(a_it, p.csr_val.get(), xcv, EpiBStore{ax.get(), row_inst.get(), S.done}, st);
+        launch_spmv_t<double, T, double>(at_it, p.csc_val.get(), ycv, EpiBStore{aty.get(), col_inst.get(), S.done}, st);
+        k_bkkt<T><<<count, kThreads, 0, st>>>(d_roff.get(), d_coff.get(), ax.get(), aty.get(), xcv, ycv,
+                                              p.row_lower.get(), p.row_upper.get(), lp.row_lower.get(),
+                                              lp.row_upper.get(), p.row_scale.get(), p.c.get(), lp.col_lower.get(),
+                                              lp.col_upper.get(), p.col_scale.get(), x_last.get(), y_last.get(),
+                                              part.get(), S);
         BControl c2 = bc;
         c2.len = len;
+        c2.pass32 = sizeof(T) == 4 ? 1 : 0;
         k_bcontrol<<<(count + 127) / 128, 128, 0, st>>>(part.get(), c2, S);
-        k_brestart<<<grid_for(mx), kThreads, 0, st>>>(m, n, row_inst.get(), col_inst.get(), xc.get(), yc.get(), x.get(),
-                                                      x0.get(), y.get(), y0.get(), x_last.get(), y_last.get(), S);
+        k_brestart<T><<<grid_for(mx), kThreads, 0, st>>>(m, n, row_inst.get(), col_inst.get(), xcv, ycv, xv, x0v, yv,
+                                                         y0v, x_last.get(), y_last.get(), S);
         k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get());
         note_launch(4);
     };
@@ -695,31 +833,50 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     const int64_t max_iter = o.iteration_limit;
     int64_t launched = 0;
     bool time_out = false;
-    while (launched < max_iter) {
-        const int64_t remaining = max_iter - launched;
-        const int len = static_cast<int>(remaining < K ? remaining : K);
-        if (len == K) {
-            if (!guard.e) {
-                const int64_t before = launch_count();
-                VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                enqueue_chunk(len);
-                VJ_CUDA(cudaStreamEndCapture(st, &guard.g));
-                VJ_CUDA(cudaGraphInstantiate(&guard.e, guard.g, 0));
-                graph_kernels = launch_count() - before;
-                launch_count() = before;
+    // Runs chunks of one pass until no instance is left in it or a limit is reached.
+    auto run_pass = [&](auto tag) -> vajra_status {
+        using T = decltype(tag);
+        const int k = sizeof(T) == 4 ? 0 : 1;
+        while (launched < max_iter) {
+            const int64_t remaining = max_iter - launched;
+            const int len = static_cast<int>(remaining < K ? remaining : K);
+            if (len == K) {
+                if (!guard.e[k]) {
+                    const int64_t before = launch_count();
+                    VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                    chunk(tag, len);
+                    VJ_CUDA(cudaStreamEndCapture(st, &guard.g[k]));
+                    VJ_CUDA(cudaGraphInstantiate(&guard.e[k], guard.g[k], 0));
+                    graph_kernels[k] = launch_count() - before;
+                    launch_count() = before;
+                }
+                VJ_CUDA(cudaGraphLaunch(guard.e[k], st));
+                note_launch(graph_kernels[k]);
+            } else {
+                chunk(tag, len);
+                VJ_LAUNCH_CHECK();
             }
-            VJ_CUDA(cudaGraphLaunch(guard.e, st));
-            note_launch(graph_kernels);
-        } else {
-            enqueue_chunk(len);
-            VJ_LAUNCH_CHECK();
+            launched += len;
+            VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+            VJ_CUDA(cudaStreamSynchronize(st));
+            if (hc->active == 0) break;
+            if (seconds_since(t_start) > o.time_limit) { time_out = true; break; }
         }
-        launched += len;
+        return VAJRA_OK;
+    };
+    if (mixed) {
+        VJ_TRY(run_pass(float{}));
+        k_bhandover<<<grid_for(mx), kThreads, 0, st>>>(m, n, row_inst.get(), col_inst.get(), xc32.get(), yc32.get(),
+                                                       x.get(), x0.get(), xc.get(), x_last.get(), y.get(), y0.get(),
+                                                       yc.get(), y_last.get(), S.status);
+        k_bhandover_state<<<(count + 127) / 128, 128, 0, st>>>(count, o.reflection, S);
+        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get());
+        VJ_LAUNCH_CHECK();
+        note_launch(3);
         VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
         VJ_CUDA(cudaStreamSynchronize(st));
-        if (hc->active == 0) break;
-        if (seconds_since(t_start) > o.time_limit) { time_out = true; break; }
     }
+    if (!time_out && (!mixed || hc->active > 0)) VJ_TRY(run_pass(double{}));
 
     // ---- post-processing -------------------------------------------------------------------
     DeviceBuffer<double> x_out, y_out, row_value, col_dual, objs;
@@ -738,9 +895,9 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     note_launch(3);
     VJ_LAUNCH_CHECK();
     timer.stop(st);
-    std::vector<double> hx(n), hy(m), hrv(m), hcd(n), hobj(count), hd(16 * static_cast<size_t>(count));
-    std::vector<long long> hl(2 * static_cast<size_t>(count));
-    std::vector<int> hi(4 * static_cast<size_t>(count));
+    std::vector<double> hx(n), hy(m), hrv(m), hcd(n), hobj(count), hd(18 * static_cast<size_t>(count));
+    std::vector<long long> hl(3 * static_cast<size_t>(count));
+    std::vector<int> hi(5 * static_cast<size_t>(count));
     VJ_CUDA(cudaMemcpyAsync(hx.data(), x_out.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaMemcpyAsync(hy.data(), y_out.get(), sizeof(double) * m, cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaMemcpyAsync(hrv.data(), row_value.get(), sizeof(double) * m, cudaMemcpyDeviceToHost, st));
@@ -775,8 +932,8 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
         r->sigma = field(3, i);
         r->spectral_norm_estimate = field(15, i);
         r->converged = r->status == 1 ? 1 : 0;
-        r->fp64_iterations = r->iterations;
-        r->fp32_iterations = 0;
+        r->fp32_iterations = hl[2 * static_cast<size_t>(count) + i];
+        r->fp64_iterations = r->iterations - r->fp32_iterations;
         r->spmv_group_a = a.group;
         r->spmv_group_at = at.group;
         std::snprintf(r->status_message, sizeof(r->status_message), "%s",
