@@ -416,6 +416,26 @@ __global__ void k_bhandover_state(int count, double gamma64, BatchArrays S) {
     instance_weights(S, i);
 }
 
+// Packing: an instance's column pointers (copied as they are, starting at 0) shifted by its
+// first entry; then its row indices shifted by its first row (the pointers are final by then).
+__global__ void k_bshift_cols(int n, const int* __restrict__ col_inst, const int64_t* __restrict__ zoff,
+                              int64_t* __restrict__ col_ptr) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) col_ptr[j] += zoff[col_inst[j]];
+}
+__global__ void k_bshift_rows(int n, const int* __restrict__ col_inst, const int64_t* __restrict__ roff,
+                              const int64_t* __restrict__ col_ptr, int32_t* __restrict__ row_idx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int32_t r0 = static_cast<int32_t>(roff[col_inst[j]]);
+    for (int64_t k = col_ptr[j]; k < col_ptr[j + 1]; ++k) row_idx[k] += r0;
+}
+__global__ void k_bmin_c(int n, const int* __restrict__ col_inst, const int* __restrict__ sense,
+                         const double* __restrict__ c, double* __restrict__ cmin) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) cmin[j] = sense[col_inst[j]] ? -c[j] : c[j];
+}
+
 template <typename To>
 __global__ void k_bconvert(int64_t n, const double* __restrict__ src, To* __restrict__ dst) {
     for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
@@ -547,7 +567,10 @@ vajra_status up(DeviceBuffer<T>& d, const std::vector<T>& h, cudaStream_t st) {
 vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajra_result* results,
                        cudaStream_t st, double* device_time) {
     const auto t_start = Clock::now();
-    // ---- host packing (block-diagonal CSC) ----------------------------------------------
+    // ---- packing (block-diagonal CSC), straight into the device buffers ----------------------
+    // Each instance's arrays are copied to their slots of the packed arrays as they are; two
+    // kernels then shift its column pointers by its first entry and its row indices by its
+    // first row.  No host copy of the entries is made.
     std::vector<int64_t> roff(count + 1, 0), coff(count + 1, 0), zoff(count + 1, 0);
     for (int i = 0; i < count; ++i) {
         roff[i + 1] = roff[i] + lps[i].num_rows;
@@ -557,58 +580,67 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     const int64_t M = roff[count], N = coff[count], NNZ = zoff[count];
     if (M >= (1LL << 31) || N >= (1LL << 31)) { set_error("packed batch exceeds 2^31 rows or columns"); return VAJRA_ERR_INVALID_ARGUMENT; }
     const int m = static_cast<int>(M), n = static_cast<int>(N);
-    vajra_lp packed{};
-    std::vector<int64_t> cp(n + 1);
-    std::vector<int32_t> ri(NNZ);
-    std::vector<double> vals(NNZ), c(n), cl(n), cu(n), rl(m), ru(m), offsets(count);
+    std::vector<double> offsets(count);
     std::vector<int> sense(count);
     for (int i = 0; i < count; ++i) {
-        const vajra_lp& L = lps[i];
-        const int64_t c0 = coff[i], r0 = roff[i], z0 = zoff[i];
-        for (int j = 0; j < L.num_cols; ++j) cp[c0 + j] = z0 + L.col_ptr[j];
-        for (int64_t k = 0; k < L.nnz; ++k) ri[z0 + k] = static_cast<int32_t>(r0 + L.row_idx[k]);
-        if (L.nnz) std::memcpy(&vals[z0], L.values, sizeof(double) * L.nnz);
-        if (L.num_cols) {
-            std::memcpy(&c[c0], L.c, sizeof(double) * L.num_cols);
-            std::memcpy(&cl[c0], L.col_lower, sizeof(double) * L.num_cols);
-            std::memcpy(&cu[c0], L.col_upper, sizeof(double) * L.num_cols);
-        }
-        if (L.num_rows) {
-            std::memcpy(&rl[r0], L.row_lower, sizeof(double) * L.num_rows);
-            std::memcpy(&ru[r0], L.row_upper, sizeof(double) * L.num_rows);
-        }
-        sense[i] = L.sense;
-        offsets[i] = L.objective_offset;
+        sense[i] = lps[i].sense;
+        offsets[i] = lps[i].objective_offset;
     }
-    cp[n] = NNZ;
-    packed.num_rows = m; packed.num_cols = n; packed.nnz = NNZ;
-    packed.col_ptr = cp.data(); packed.row_idx = ri.data(); packed.values = vals.data();
-    packed.c = c.data(); packed.col_lower = cl.data(); packed.col_upper = cu.data();
-    packed.row_lower = rl.data(); packed.row_upper = ru.data();
-    // maximisation instances are negated here (the packed problem is a minimisation)
-    std::vector<double> cmin(c);
-    for (int i = 0; i < count; ++i)
-        if (sense[i]) for (int64_t j = coff[i]; j < coff[i + 1]; ++j) cmin[j] = -cmin[j];
+    auto mark = [&](const char* what) {
+        if (!o.verbose) return;
+        cudaStreamSynchronize(st);
+        std::fprintf(stderr, "[vajra] batch %-22s %8.1f ms\n", what, 1e3 * seconds_since(t_start));
+    };
 
     StreamTimer timer;
     timer.start(st);
     DeviceLp lp;
-    VJ_TRY(upload_lp(&packed, lp, st));
-    DeviceBuffer<double> d_cmin;
-    VJ_TRY(up(d_cmin, cmin, st));
-    DeviceBuffer<int64_t> d_roff, d_coff;
+    lp.m = m;
+    lp.n = n;
+    lp.nnz = NNZ;
+    VJ_TRY(lp.col_ptr.alloc(static_cast<size_t>(n) + 1));
+    VJ_TRY(lp.row_idx.alloc(static_cast<size_t>(NNZ)));
+    VJ_TRY(lp.values.alloc(static_cast<size_t>(NNZ)));
+    for (auto* b : {&lp.c, &lp.col_lower, &lp.col_upper}) VJ_TRY(b->alloc(n));
+    for (auto* b : {&lp.row_lower, &lp.row_upper}) VJ_TRY(b->alloc(m));
+    auto put = [&](auto* dst, const auto* src, int64_t k) -> vajra_status {
+        if (k > 0) VJ_CUDA(cudaMemcpyAsync(dst, src, sizeof(*src) * k, cudaMemcpyHostToDevice, st));
+        return VAJRA_OK;
+    };
+    for (int i = 0; i < count; ++i) {
+        const vajra_lp& L = lps[i];
+        const int64_t c0 = coff[i], r0 = roff[i], z0 = zoff[i];
+        VJ_TRY(put(lp.col_ptr.get() + c0, L.col_ptr, L.num_cols));
+        VJ_TRY(put(lp.row_idx.get() + z0, L.row_idx, L.nnz));
+        VJ_TRY(put(lp.values.get() + z0, L.values, L.nnz));
+        VJ_TRY(put(lp.c.get() + c0, L.c, L.num_cols));
+        VJ_TRY(put(lp.col_lower.get() + c0, L.col_lower, L.num_cols));
+        VJ_TRY(put(lp.col_upper.get() + c0, L.col_upper, L.num_cols));
+        VJ_TRY(put(lp.row_lower.get() + r0, L.row_lower, L.num_rows));
+        VJ_TRY(put(lp.row_upper.get() + r0, L.row_upper, L.num_rows));
+    }
+    VJ_TRY(put(lp.col_ptr.get() + n, &NNZ, 1));
+    DeviceBuffer<int64_t> d_roff, d_coff, d_zoff;
     DeviceBuffer<int> d_sense, row_inst, col_inst;
-    DeviceBuffer<double> d_offsets;
+    DeviceBuffer<double> d_offsets, d_cmin;
     VJ_TRY(up(d_roff, roff, st));
     VJ_TRY(up(d_coff, coff, st));
+    VJ_TRY(up(d_zoff, zoff, st));
     VJ_TRY(up(d_sense, sense, st));
     VJ_TRY(up(d_offsets, offsets, st));
     VJ_TRY(row_inst.alloc(m));
     VJ_TRY(col_inst.alloc(n));
+    VJ_TRY(d_cmin.alloc(n));
     k_fill_inst<<<count, kThreads, 0, st>>>(M, d_roff.get(), count, row_inst.get());
     k_fill_inst<<<count, kThreads, 0, st>>>(N, d_coff.get(), count, col_inst.get());
+    k_bshift_cols<<<grid_for(n), kThreads, 0, st>>>(n, col_inst.get(), d_zoff.get(), lp.col_ptr.get());
+    k_bshift_rows<<<grid_for(n), kThreads, 0, st>>>(n, col_inst.get(), d_roff.get(), lp.col_ptr.get(),
+                                                    lp.row_idx.get());
+    // the packed problem is a minimisation: maximisation instances' objectives are negated
+    k_bmin_c<<<grid_for(n), kThreads, 0, st>>>(n, col_inst.get(), d_sense.get(), lp.c.get(), d_cmin.get());
     VJ_LAUNCH_CHECK();
-    note_launch(2);
+    note_launch(5);
+    mark("packed on the device");
 
     // ---- set-up on the packed problem --------------------------------------------------
     Prepared p;
@@ -742,6 +774,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
         cudaEventDestroy(e1);
     }
 
+    mark("set-up");
     // Iteration views in list mode: only blocks of unfinished instances run (rebuilt at the
     // start of every chunk, after the previous check decided which instances are done).
     int sms = 148;
@@ -877,6 +910,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
         VJ_CUDA(cudaStreamSynchronize(st));
     }
     if (!time_out && (!mixed || hc->active > 0)) VJ_TRY(run_pass(double{}));
+    mark("iterations");
 
     // ---- post-processing -------------------------------------------------------------------
     DeviceBuffer<double> x_out, y_out, row_value, col_dual, objs;
@@ -908,6 +942,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     VJ_CUDA(cudaMemcpyAsync(hi.data(), di.get(), sizeof(int) * hi.size(), cudaMemcpyDeviceToHost, st));
     VJ_CUDA(cudaStreamSynchronize(st));
     if (device_time) *device_time = timer.seconds();
+    mark("post-processing, copies");
     auto field = [&](int q, int i) { return hd[static_cast<size_t>(q) * count + i]; };
     for (int i = 0; i < count; ++i) {
         vajra_result* r = &results[i];
