@@ -11,9 +11,11 @@
 // belong only to finished instances are skipped before any load, so the work shrinks as
 // instances converge.  Every check interval one CTA per instance reduces that instance's KKT
 // terms, one thread per instance runs the restart / primal-weight / termination logic
-// (same rules as the single-LP solver), and the host reads one counter of active
-// instances.  A chunk of iterations plus its check is one CUDA graph launch; no kernel waits
-// on another kernel, so nothing in this path can spin.
+// (same rules as the single-LP solver), and one thread counts the active instances.  A pass
+// is one CUDA graph whose WHILE node repeats the chunk (iterations plus check) on the device
+// while an instance is active, up to kChunksPerLaunch chunks a launch; the host reads the
+// counters once per launch.  No kernel waits on another kernel, so nothing in this path can
+// spin, and the loop's chunk budget ends every launch.
 //
 // Differences from solving the instances one by one: the Ruiz stopping test is evaluated
 // over the packed matrix (all instances take the same number of passes), and the power
@@ -49,10 +51,18 @@ constexpr int kBHist = 32;
 // Status of an instance that left the FP32 pass for the FP64 one (internal, never reported).
 constexpr int kBHandover = 100;
 
+// Read by the host after every launch of the pass graph.  `left` bounds the chunks one launch
+// may run (the host writes it before the launch, the loop counts it down); `chunks` counts the
+// chunks the loop ran.
 struct BatchCounters {
     int active;
-    int pad;
+    int left;
+    long long chunks;
 };
+
+// Chunks one launch of a pass graph may run before the host looks at the counters again
+// (time limit, iteration limit): 2048 iterations at 64 per chunk.
+constexpr int kChunksPerLaunch = 32;
 
 __device__ __forceinline__ void instance_weights(const BatchArrays& S, int i) {
     const long long kb = S.k_base[i];
@@ -358,12 +368,25 @@ __global__ void k_bcontrol(const double* __restrict__ part, BControl cp, BatchAr
     instance_weights(S, i);
 }
 
-__global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restrict__ done, BatchCounters* out) {
+// Counts the unfinished instances.  Inside the WHILE body of a pass graph (`loop` = 1) it also
+// decides whether the body runs again: only while an instance is active and the launch's chunk
+// budget is not spent, so every launch ends after at most `left` chunks whatever the iterates do.
+__global__ void __launch_bounds__(1024) k_bcount(int count, const int* __restrict__ done, BatchCounters* out,
+                                                 cudaGraphConditionalHandle again, int loop) {
     __shared__ double red[32];
     double v[1] = {0.0};
     for (int i = threadIdx.x; i < count; i += blockDim.x) v[0] += done[i] ? 0.0 : 1.0;
     block_reduce<OpSum, double, 1>(v, red);
-    if (threadIdx.x == 0) out->active = static_cast<int>(v[0]);
+    if (threadIdx.x == 0) {
+        const int active = static_cast<int>(v[0]);
+        out->active = active;
+        if (loop) {
+            const int left = out->left - 1;
+            out->left = left;
+            out->chunks += 1;
+            cudaGraphSetConditional(again, active > 0 && left > 0 ? 1u : 0u);
+        }
+    }
 }
 
 template <typename T>
@@ -790,8 +813,10 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
 
     DeviceBuffer<BatchCounters> counters;
     VJ_TRY(counters.alloc(1));
+    VJ_CUDA(cudaMemsetAsync(counters.get(), 0, sizeof(BatchCounters), st));
     BatchCounters* hc = nullptr;
     VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hc), sizeof(BatchCounters)));
+    std::memset(hc, 0, sizeof(BatchCounters));
     struct Guard {
         BatchCounters* h; cudaGraph_t g[2] = {nullptr, nullptr}; cudaGraphExec_t e[2] = {nullptr, nullptr};
         ~Guard() {
@@ -826,7 +851,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     const PassBuffers pb32{p.csr_val32.get(), p.csc_val32.get(), c32.get(), cl32.get(), cu32.get(), rl32.get(),
                            ru32.get(), x32.get(), x0_32.get(), xb32.get(), xc32.get(), y32.get(), y0_32.get(),
                            yc32.get()};
-    auto chunk = [&](auto tag, int len) {
+    auto chunk = [&](auto tag, int len, cudaGraphConditionalHandle again, int loop) {
         using T = decltype(tag);
         const PassBuffers& b = sizeof(T) == 4 ? pb32 : pb64;
         const T* csr = static_cast<const T*>(b.csr);
@@ -859,39 +884,62 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
         k_bcontrol<<<(count + 127) / 128, 128, 0, st>>>(part.get(), c2, S);
         k_brestart<T><<<grid_for(mx), kThreads, 0, st>>>(m, n, row_inst.get(), col_inst.get(), xcv, ycv, xv, x0v, yv,
                                                          y0v, x_last.get(), y_last.get(), S);
-        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get());
+        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get(), again, loop);
         note_launch(4);
     };
 
     const int64_t max_iter = o.iteration_limit;
     int64_t launched = 0;
     bool time_out = false;
-    // Runs chunks of one pass until no instance is left in it or a limit is reached.
+    // Runs one pass until no instance is left in it or a limit is reached.  Full chunks run in
+    // the pass graph: a WHILE node whose body is one chunk, repeated on the device while an
+    // instance is active, at most `left` times a launch.  A last partial chunk (iteration
+    // limit not a multiple of K) is launched directly.
     auto run_pass = [&](auto tag) -> vajra_status {
         using T = decltype(tag);
         const int k = sizeof(T) == 4 ? 0 : 1;
         while (launched < max_iter) {
             const int64_t remaining = max_iter - launched;
-            const int len = static_cast<int>(remaining < K ? remaining : K);
-            if (len == K) {
+            if (remaining >= K) {
                 if (!guard.e[k]) {
+                    VJ_CUDA(cudaGraphCreate(&guard.g[k], 0));
+                    cudaGraphConditionalHandle again;
+                    VJ_CUDA(cudaGraphConditionalHandleCreate(&again, guard.g[k], 1, cudaGraphCondAssignDefault));
+                    cudaGraphNodeParams np{};
+                    np.type = cudaGraphNodeTypeConditional;
+                    np.conditional.handle = again;
+                    np.conditional.type = cudaGraphCondTypeWhile;
+                    np.conditional.size = 1;
+                    cudaGraphNode_t loop_node;
+                    VJ_CUDA(cudaGraphAddNode(&loop_node, guard.g[k], nullptr, 0, &np));
                     const int64_t before = launch_count();
-                    VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                    chunk(tag, len);
-                    VJ_CUDA(cudaStreamEndCapture(st, &guard.g[k]));
+                    VJ_CUDA(cudaStreamBeginCaptureToGraph(st, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                          cudaStreamCaptureModeThreadLocal));
+                    chunk(tag, K, again, 1);
+                    cudaGraph_t body = nullptr;
+                    VJ_CUDA(cudaStreamEndCapture(st, &body));
                     VJ_CUDA(cudaGraphInstantiate(&guard.e[k], guard.g[k], 0));
                     graph_kernels[k] = launch_count() - before;
                     launch_count() = before;
                 }
+                const int64_t budget = remaining / K < kChunksPerLaunch ? remaining / K : kChunksPerLaunch;
+                const long long chunks_before = hc->chunks;
+                hc->left = static_cast<int>(budget);
+                VJ_CUDA(cudaMemcpyAsync(&counters.get()->left, &hc->left, sizeof(int), cudaMemcpyHostToDevice, st));
                 VJ_CUDA(cudaGraphLaunch(guard.e[k], st));
-                note_launch(graph_kernels[k]);
+                VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+                VJ_CUDA(cudaStreamSynchronize(st));
+                const long long ran = hc->chunks - chunks_before;
+                note_launch(graph_kernels[k] * ran);
+                launched += ran * K;
+                if (ran < 1 || ran > budget) return VAJRA_ERR_INTERNAL;   // the loop runs 1..budget chunks
             } else {
-                chunk(tag, len);
+                chunk(tag, static_cast<int>(remaining), cudaGraphConditionalHandle{}, 0);
                 VJ_LAUNCH_CHECK();
+                launched += remaining;
+                VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
+                VJ_CUDA(cudaStreamSynchronize(st));
             }
-            launched += len;
-            VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
-            VJ_CUDA(cudaStreamSynchronize(st));
             if (hc->active == 0) break;
             if (seconds_since(t_start) > o.time_limit) { time_out = true; break; }
         }
@@ -903,7 +951,7 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
                                                        x.get(), x0.get(), xc.get(), x_last.get(), y.get(), y0.get(),
                                                        yc.get(), y_last.get(), S.status);
         k_bhandover_state<<<(count + 127) / 128, 128, 0, st>>>(count, o.reflection, S);
-        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get());
+        k_bcount<<<1, 1024, 0, st>>>(count, S.done, counters.get(), cudaGraphConditionalHandle{}, 0);
         VJ_LAUNCH_CHECK();
         note_launch(3);
         VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
