@@ -197,6 +197,14 @@ int sm_count() {
     return sms;
 }
 
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("VAJRA_PDL");
+        return !(e && std::strcmp(e, "0") == 0);
+    }();
+    return on;
+}
+
 void copy_out_vector(double* dst, const double* dev, int count, cudaStream_t st) {
     if (dst && count > 0) cudaMemcpyAsync(dst, dev, sizeof(double) * count, cudaMemcpyDeviceToHost, st);
 }

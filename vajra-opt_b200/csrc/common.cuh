@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 
 #include "vajra_pdhg.h"
 
@@ -46,6 +47,42 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
     if (g < 1) g = 1;
     if (g > cap) g = cap;
     return static_cast<unsigned>(g);
+}
+
+// Programmatic dependent launch.  The SpMV kernels are launched with programmatic stream
+// serialization: the next kernel's CTAs may be scheduled while the previous kernel in the
+// stream is still draining, which hides most of the launch gap between the two SpMVs of an
+// iteration when the SpMVs themselves take a few microseconds.  Every kernel launched that way
+// runs pdl_enter() before anything else: griddepcontrol.wait returns once the previous kernel
+// has completed and its writes are visible, so nothing is read or written early, and a kernel
+// that then returns at once has still waited (the kernel after it sees everything before it).
+// launch_dependents then lets the next kernel be scheduled.  In a kernel launched without the
+// attribute both instructions return at once.  VAJRA_PDL=0 in the environment launches the
+// SpMV kernels without it.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// False when VAJRA_PDL=0 (read once per process).
+bool pdl_enabled();
+
+// <<<grid, block, smem, st>>> with programmatic stream serialization; errors are left for
+// cudaGetLastError, as with <<<>>>.
+template <typename... Params, typename... Args>
+inline void launch_chained(void (*kernel)(Params...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                           Args&&... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // Device blocks go through a process-wide cache keyed by (device, size class): a released

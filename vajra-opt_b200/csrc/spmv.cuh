@@ -112,6 +112,7 @@ template <typename V, bool ZERO_DROP, class Epi>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_seq(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
            const V* __restrict__ val, const V* __restrict__ x, Epi epi) {
+    pdl_enter();
     if (!epi.active()) return;
     const int row = blockIdx.x * blockDim.x + threadIdx.x;
     if (row >= rows) return;
@@ -163,6 +164,7 @@ k_spmv_vec(int rows, const int64_t* __restrict__ ptr, const int32_t* __restrict_
            const VV* __restrict__ val, const VX* __restrict__ x, int64_t long_len,
            const int32_t* __restrict__ long_rows, int vec_blocks, const int32_t* __restrict__ blk_list,
            const int* __restrict__ blk_count, Epi epi) {
+    pdl_enter();
     if (!epi.active()) return;
     if (static_cast<int>(blockIdx.x) >= vec_blocks) {
         // One CTA per long row.
@@ -319,6 +321,7 @@ k_spmv_rowblock(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx
     __shared__ int med_rows[(2 * KT) / MR + 1];
     __shared__ int n_med;
     __shared__ Acc red[32];
+    pdl_enter();
     if (!epi.active()) return;
     if (static_cast<int>(blockIdx.x) >= nb) {
         const int row = long_rows[blockIdx.x - nb];
@@ -461,6 +464,7 @@ k_spmv_sell(int rows, int slices, const int64_t* __restrict__ ptr, const int32_t
             const int32_t* __restrict__ long_rows, int n_long, const uint8_t* __restrict__ sell_len,
             const int64_t* __restrict__ sell_off,
             const int32_t* __restrict__ sell_idx, const VV* __restrict__ sell_val, const VX* __restrict__ x, Epi epi) {
+    pdl_enter();
     if (!epi.active()) return;
     int b = static_cast<int>(blockIdx.x);
     if (b < n_vlong) {
@@ -517,6 +521,7 @@ k_spmv_sell_hot(int rows, int slices, const int64_t* __restrict__ ptr, const int
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Acc red[32];
     VX* xs = reinterpret_cast<VX*>(smem_raw);
+    pdl_enter();
     if (!epi.active()) return;   // uniform over the grid (device state)
     // x[0, hot): 16-byte loads (x is a device allocation, 256-byte aligned; hot is a multiple
     // of the vector width), written by the previous kernel, so a plain load
@@ -597,9 +602,9 @@ inline void launch_sell(const CsrView& a, const VV* csr_val, const VV* sell_val,
     constexpr int kWarps = kThreads / 32;
     const int blocks = a.sell_n_vlong + (a.sell_n_long + kWarps - 1) / kWarps + sell_block_count(a);
     if (blocks <= 0) return;
-    k_spmv_sell<VV, VX, Acc, Epi, MB><<<blocks, kThreads, 0, st>>>(
-        a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
-        a.sell_n_long, a.sell_len, a.sell_off, a.sell_idx, sell_val, x, epi);
+    launch_chained(k_spmv_sell<VV, VX, Acc, Epi, MB>, blocks, kThreads, 0, st,
+                   a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
+                   a.sell_n_long, a.sell_len, a.sell_off, a.sell_idx, sell_val, x, epi);
     note_launch();
 }
 
@@ -637,9 +642,9 @@ inline void launch_sell_hot(const CsrView& a, const VV* csr_val, const VV* sell_
     const int hot = sell_hot_extent<VX>(a.cols);
     // a vector shorter than the 16-byte padding of its allocation is still read whole (the
     // buffers carry 16 spare elements, so the rounded-up extent stays inside the allocation)
-    k_spmv_sell_hot<VV, VX, Acc, Epi><<<grid, kSellHotThreads, static_cast<size_t>(hot) * sizeof(VX), st>>>(
-        a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
-        a.sell_n_long, a.sell_len, a.sell_off, a.sell_idx, sell_val, x, hot, epi);
+    launch_chained(k_spmv_sell_hot<VV, VX, Acc, Epi>, grid, kSellHotThreads, static_cast<size_t>(hot) * sizeof(VX), st,
+                   a.rows, a.sell_slices, a.ptr, a.idx, csr_val, a.sell_vlong_rows, a.sell_n_vlong, a.sell_long_rows,
+                   a.sell_n_long, a.sell_len, a.sell_off, a.sell_idx, sell_val, x, hot, epi);
     note_launch();
 }
 
@@ -656,8 +661,8 @@ inline void launch_rowblock(const CsrView& a, const VV* val, const VX* x, Epi ep
     const int nb = a.blk_list ? a.blk_grid : a.nb;
     constexpr int MB = U == 1 ? rowblock_min_blocks<VV>() : (sizeof(VV) == 4 ? 6 : 4);
     constexpr bool PRE = U == 1 || sizeof(VV) != 4;
-    k_spmv_rowblock<VV, VX, Acc, Epi, MB, U, kTile, kMediumRow, PRE><<<nb + a.rb_n_long, kThreads, smem, st>>>(
-        a.ptr, a.idx, val, x, a.tiles, nb, a.rb_long_rows, a.blk_list, a.blk_count, epi);
+    launch_chained(k_spmv_rowblock<VV, VX, Acc, Epi, MB, U, kTile, kMediumRow, PRE>, nb + a.rb_n_long, kThreads, smem,
+                   st, a.ptr, a.idx, val, x, a.tiles, nb, a.rb_long_rows, a.blk_list, a.blk_count, epi);
     note_launch();
 }
 
@@ -667,8 +672,8 @@ inline int vec_block_count(int rows, int G) { return static_cast<int>(grid_for(s
 template <typename VV, typename VX, typename Acc, int G, class Epi>
 inline void launch_vec_g(const CsrView& a, const VV* val, const VX* x, Epi epi, cudaStream_t st) {
     const int vec_blocks = a.blk_list ? a.blk_grid : vec_block_count(a.rows, G);
-    k_spmv_vec<VV, VX, Acc, G, Epi><<<vec_blocks + a.n_long, kThreads, 0, st>>>(
-        a.rows, a.ptr, a.idx, val, x, a.long_len, a.long_rows, vec_blocks, a.blk_list, a.blk_count, epi);
+    launch_chained(k_spmv_vec<VV, VX, Acc, G, Epi>, vec_blocks + a.n_long, kThreads, 0, st,
+                   a.rows, a.ptr, a.idx, val, x, a.long_len, a.long_rows, vec_blocks, a.blk_list, a.blk_count, epi);
     note_launch();
 }
 
@@ -706,7 +711,7 @@ inline void launch_spmv(const CsrView& a, const V* val, const V* x, Epi epi, cud
 template <typename V, bool ZERO_DROP, class Epi>
 inline void launch_spmv_exact(const CsrView& a, const V* val, const V* x, Epi epi, cudaStream_t st) {
     if (a.rows <= 0) return;
-    k_spmv_seq<V, ZERO_DROP, Epi><<<grid_for(a.rows), kThreads, 0, st>>>(a.rows, a.ptr, a.idx, val, x, epi);
+    launch_chained(k_spmv_seq<V, ZERO_DROP, Epi>, grid_for(a.rows), kThreads, 0, st, a.rows, a.ptr, a.idx, val, x, epi);
     note_launch();
 }
 
