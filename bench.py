@@ -638,11 +638,12 @@ def run(args, world, rank, local, dist):
     e2e = None
     if not args.no_e2e:
         barrier()
-        e2e_times = []
+        e2e_times, e2e_calls = [], []
         for _ in range(args.steps):
             t0 = time.perf_counter()
             r = V.solve(plp, precision=V.PREC_MIXED, device=local, degree_order=args.degree_order, **knobs)
             e2e_times.append(time.perf_counter() - t0)
+            e2e_calls.append([round(e2e_times[-1], 4), round(r["device_time_sec"], 4), round(r["setup_time_sec"], 4)])
         barrier()
         h2d = 8 * (lp.num_cols + 1) + 12 * lp.nnz + 8 * (3 * lp.num_cols + 2 * lp.num_rows)
         d2h = 8 * (2 * lp.num_cols + 2 * lp.num_rows)
@@ -650,6 +651,7 @@ def run(args, world, rank, local, dist):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "status": r["status_name"], "rel_kkt": r["rel_kkt"],
                "calls_min_max_s": [round(min(e2e_times), 4), round(max(e2e_times), 4)],
+               "calls_wall_device_setup_s": e2e_calls,
                "last_setup_s": round(r["setup_time_sec"], 4), "last_device_s": round(r["device_time_sec"], 4)}
         if cold is not None:
             e2e["cold_first_call"] = cold
