@@ -109,10 +109,12 @@ def batch_line(args, world=1, rank=0, dist=None, sequential=True):
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    mine, res, summaries = S.solve_batch_sharded(lps, rank, world, dist)
-    torch.cuda.synchronize()
-    batch_wall = S.max_over_ranks(time.perf_counter() - t0, dist, dev)
+    with ClockSampler(torch.cuda.current_device(), args.clock_period_ms) as clocks:
+        t0 = time.perf_counter()
+        mine, res, summaries = S.solve_batch_sharded(lps, rank, world, dist)
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+    batch_wall = S.max_over_ranks(t_batch, dist, dev)
     batch_dev = S.max_over_ranks(res[0]["device_time_sec"] if res else 0.0, dist, dev)
     ok = sum(s["status_name"] == "OPTIMAL" for s in summaries)
     worst_kkt = S.max_over_ranks(max((relative_kkt(lps[i], r["x"], r["y"])["rel_kkt"] for i, r in zip(mine, res)),
@@ -128,6 +130,7 @@ def batch_line(args, world=1, rank=0, dist=None, sequential=True):
                       "iterations_p50_p90_p99": [int(np.percentile(iters, q)) for q in (50, 90, 99)],
                       "busy_fraction": sum(k * lp.nnz for k, lp in zip(iters, lps)) / (max(iters) * nnz),
                       "spmv_groups": [res[0]["spmv_group_a"], res[0]["spmv_group_at"]] if res else None},
+            "clocks": clocks.summary(),
             "data": "synthetic",
             "config": {"workload": f"{len(lps)} LPs, m log-uniform on [100, 20000], n = round(U[2,3] m), "
                                    f"nnz per column U{{4..12}}, planted optima, seed 3",
@@ -141,15 +144,17 @@ def batch_line(args, world=1, rank=0, dist=None, sequential=True):
                               "max_iterations": max(r["iterations"] for r in rb)}
         nseq = len(lps) if args.batch_sequential < 0 else min(args.batch_sequential, len(lps))
         V.solve(lps[0], precision=V.PREC_FP64)
-        seq_times, seq_ok = [], 0
-        for lp in lps[:nseq]:
-            t0 = time.perf_counter()
-            r = V.solve(lp, precision=V.PREC_FP64)
-            seq_times.append(time.perf_counter() - t0)
-            seq_ok += r["status_name"] == "OPTIMAL"
+        seq_times, seq_dev, seq_ok = [], [], 0
+        with ClockSampler(torch.cuda.current_device(), args.clock_period_ms) as seq_clocks:
+            for lp in lps[:nseq]:
+                t0 = time.perf_counter()
+                r = V.solve(lp, precision=V.PREC_FP64)
+                seq_times.append(time.perf_counter() - t0)
+                seq_dev.append(r["device_time_sec"])
+                seq_ok += r["status_name"] == "OPTIMAL"
         seq_total = sum(seq_times) * len(lps) / max(1, nseq)
         line["sequential"] = {"timed": nseq, "total_s_for_all": seq_total, "solves_per_s": len(lps) / seq_total,
-                              "optimal": seq_ok}
+                              "device_s_for_timed": sum(seq_dev), "optimal": seq_ok, "clocks": seq_clocks.summary()}
         line["speedup"] = seq_total / batch_wall
     return line
 

@@ -415,3 +415,37 @@ def test_mixed_handover_continuing_the_fp32_epoch_reaches_the_optimum(cuda):
     g = V.solve(lp, precision=V.PREC_MIXED, handover_mode=1, mixed_switch_tolerance=1e-4)
     assert g["fp32_iterations"] > 0 and g["fp64_iterations"] > 0
     check_solution(lp, g, obj=lp.planted_objective)
+
+
+def test_chained_launch_changes_no_result(cuda, tmp_path):
+    """The SpMV kernels run under programmatic dependent launch by default (each waits for the
+    previous kernel's completion before its first access); VAJRA_PDL=0 launches them plainly.
+    Same LP, same launch shapes (the set-up heuristic below 2^20 entries): bit-identical
+    iterates, iteration counts and statuses in both precisions."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "plain.npz"
+    script = (
+        "import sys, numpy as np\n"
+        "import vajra_pdhg as V\n"
+        "from vajra_pdhg import workloads as W\n"
+        "lp = W.random_planted(2000, 5000, 8, seed=0)\n"
+        "res = {}\n"
+        "for name, p in (('fp64', V.PREC_FP64), ('mixed', V.PREC_MIXED)):\n"
+        "    r = V.solve(lp, precision=p)\n"
+        "    res[name + '_x'] = r['x']; res[name + '_y'] = r['y']\n"
+        "    res[name + '_it'] = np.array([r['iterations'], r['status']])\n"
+        f"np.savez({str(out)!r}, **res)\n")
+    env = dict(os.environ, VAJRA_PDL="0",
+               PYTHONPATH=os.pathsep.join([root, os.path.join(root, "vajra-opt_b200"), os.environ.get("PYTHONPATH", "")]))
+    subprocess.run([sys.executable, "-c", script], env=env, check=True, timeout=600)
+    plain = np.load(out)
+    lp = W.random_planted(2000, 5000, 8, seed=0)
+    for name, p in (("fp64", V.PREC_FP64), ("mixed", V.PREC_MIXED)):
+        r = V.solve(lp, precision=p)
+        assert r["status_name"] == "OPTIMAL"
+        assert [r["iterations"], r["status"]] == plain[name + "_it"].tolist()
+        np.testing.assert_array_equal(r["x"], plain[name + "_x"])
+        np.testing.assert_array_equal(r["y"], plain[name + "_y"])
