@@ -728,7 +728,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     VJ_TRY(spectral_norm_fast(p, m, n, 100, 1e-5, sst.get(), st));
     mark("norm estimate");
     SetupState hss{};
-    VJ_CUDA(cudaMemcpy(&hss, sst.get(), sizeof(hss), cudaMemcpyDeviceToHost));
+    VJ_CUDA(cudaMemcpyAsync(&hss, sst.get(), sizeof(hss), cudaMemcpyDeviceToHost, st));
+    VJ_CUDA(cudaStreamSynchronize(st));
     const double spectral_norm = hss.spectral_norm;
     if (!(spectral_norm > 1e-12) || !std::isfinite(spectral_norm)) {
         r->status = kStatusNumerical;

@@ -266,7 +266,8 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     if (nnz > 0) {
         VJ_TRY(spectral_norm_exact(p, m, n, 25, 1e-4, sst.get(), st));
         SetupState hs{};
-        VJ_CUDA(cudaMemcpy(&hs, sst.get(), sizeof(hs), cudaMemcpyDeviceToHost));
+        VJ_CUDA(cudaMemcpyAsync(&hs, sst.get(), sizeof(hs), cudaMemcpyDeviceToHost, st));
+        VJ_CUDA(cudaStreamSynchronize(st));
         spectral_norm = hs.spectral_norm;
     }
     const double safety = 0.95;       // clamp(0.95, 0.5, 0.99), pdhg.cpp:156
