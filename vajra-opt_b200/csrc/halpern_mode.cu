@@ -924,6 +924,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
             const CsrView& iat = ph.phase == 0 ? at32 : at64;
             if (len == K) {
                 if (!ph.exec) {
+                    const auto t_graph = Clock::now();
                     const int64_t before = launch_count();
                     VJ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                     enqueue_chunk(ph, ia, iat, a64, at64, p, lp, cb, S, len, cp, true, st);
@@ -931,6 +932,9 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
                     VJ_CUDA(cudaGraphInstantiate(&ph.exec, ph.graph, 0));
                     ph.graph_kernels = launch_count() - before;
                     launch_count() = before;
+                    if (o.verbose)
+                        std::fprintf(stderr, "[vajra] chunk graph of phase %d (%lld kernels): capture + instantiate %.2f ms\n",
+                                     ph.phase, static_cast<long long>(ph.graph_kernels), 1e3 * seconds_since(t_graph));
                 }
                 VJ_CUDA(cudaGraphLaunch(ph.exec, st));
                 note_launch(ph.graph_kernels);
@@ -984,6 +988,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         if (seconds_since(t_start) > o.time_limit) { timed_out = 1; break; }
     }
     const double iter_time = seconds_since(t_iter);
+    if (o.verbose) std::fprintf(stderr, "[vajra] iterations %.2f ms (%lld host reads)\n", 1e3 * iter_time,
+                                static_cast<long long>(h->transfers));
 
     // The returned point is the last evaluated candidate T(z) of the active precision.
     const auto t_post = Clock::now();
