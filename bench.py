@@ -144,17 +144,18 @@ def batch_line(args, world=1, rank=0, dist=None, sequential=True):
                               "max_iterations": max(r["iterations"] for r in rb)}
         nseq = len(lps) if args.batch_sequential < 0 else min(args.batch_sequential, len(lps))
         V.solve(lps[0], precision=V.PREC_FP64)
+        # no clock sampling here: each nvidia-smi query holds driver locks that the solves'
+        # per-chunk host synchronisation waits on, which would slow the baseline
         seq_times, seq_dev, seq_ok = [], [], 0
-        with ClockSampler(torch.cuda.current_device(), args.clock_period_ms) as seq_clocks:
-            for lp in lps[:nseq]:
-                t0 = time.perf_counter()
-                r = V.solve(lp, precision=V.PREC_FP64)
-                seq_times.append(time.perf_counter() - t0)
-                seq_dev.append(r["device_time_sec"])
-                seq_ok += r["status_name"] == "OPTIMAL"
+        for lp in lps[:nseq]:
+            t0 = time.perf_counter()
+            r = V.solve(lp, precision=V.PREC_FP64)
+            seq_times.append(time.perf_counter() - t0)
+            seq_dev.append(r["device_time_sec"])
+            seq_ok += r["status_name"] == "OPTIMAL"
         seq_total = sum(seq_times) * len(lps) / max(1, nseq)
         line["sequential"] = {"timed": nseq, "total_s_for_all": seq_total, "solves_per_s": len(lps) / seq_total,
-                              "device_s_for_timed": sum(seq_dev), "optimal": seq_ok, "clocks": seq_clocks.summary()}
+                              "device_s_for_timed": sum(seq_dev), "optimal": seq_ok}
         line["speedup"] = seq_total / batch_wall
     return line
 
