@@ -17,8 +17,9 @@
 // counters once per launch.  No kernel waits on another kernel, so nothing in this path can
 // spin, and the loop's chunk budget ends every launch.
 //
-// Differences from solving the instances one by one: the Ruiz stopping test is evaluated
-// over the packed matrix (all instances take the same number of passes), and the power
+// Scaling is per instance: Ruiz and Pock-Chambolle factors are local to a row or column, and
+// each instance ends its Ruiz passes on its own stopping test, so every instance is scaled
+// exactly as it would be alone.  Difference from solving the instances one by one: the power
 // iteration runs a fixed 60 rounds for every instance.
 #include <algorithm>
 #include <cmath>
@@ -675,6 +676,12 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     so.ruiz_iterations = o.ruiz_iterations > 0 ? o.ruiz_iterations : 10;
     so.pock_chambolle = o.pock_chambolle != 0;
     so.negate_c = false;
+    // each instance stops its Ruiz passes on its own test, as it would alone
+    so.instances = count;
+    so.roff = d_roff.get();
+    so.coff = d_coff.get();
+    so.row_inst = row_inst.get();
+    so.col_inst = col_inst.get();
     {
         // Upload the min-form c as the raw c for scaling, keep the caller's c for reporting.
         DeviceBuffer<double> c_raw;
@@ -932,6 +939,10 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
                 const long long ran = hc->chunks - chunks_before;
                 note_launch(graph_kernels[k] * ran);
                 launched += ran * K;
+                if (o.verbose)
+                    std::fprintf(stderr, "[vajra] batch %s pass: %lld chunks to iteration %lld, %d active, %.1f ms\n",
+                                 k == 0 ? "FP32" : "FP64", ran, static_cast<long long>(launched), hc->active,
+                                 1e3 * seconds_since(t_start));
                 if (ran < 1 || ran > budget) return VAJRA_ERR_INTERNAL;   // the loop runs 1..budget chunks
             } else {
                 chunk(tag, static_cast<int>(remaining), cudaGraphConditionalHandle{}, 0);

@@ -88,6 +88,15 @@ struct ScalingOpts {
     bool pock_chambolle = false;
     bool negate_c = false;     // maximisation
     bool pow2 = false;         // round the final factors to powers of two (exact scaling)
+    // Block-diagonal LPs (the batched solver): with instances > 0, each instance runs the Ruiz
+    // stopping test on its own rows and columns and keeps factor 1 once it has passed, so every
+    // instance is scaled exactly as it would be alone.  Offsets: instances + 1 entries each;
+    // row_inst / col_inst: the instance of every row / column.
+    int instances = 0;
+    const int64_t* roff = nullptr;
+    const int64_t* coff = nullptr;
+    const int* row_inst = nullptr;
+    const int* col_inst = nullptr;
 };
 
 // Copies the raw data into the working buffers and applies Ruiz (exactly as

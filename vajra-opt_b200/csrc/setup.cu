@@ -195,6 +195,39 @@ __global__ void k_scale_matrix(int64_t nnz, const int32_t* __restrict__ col_of, 
         v[k] = __dmul_rn(v[k], __dmul_rn(r[row_idx[k]], cs[col_of[k]]));
 }
 
+// The Ruiz convergence test of one instance of a block-diagonal LP (one CTA each): the same
+// maxima as k_row_inf / k_col_inf and k_ruiz_err over the instance's own rows and columns.
+// An instance that passes keeps factor 1 from this pass on (sticky `inst_done`).
+__global__ void __launch_bounds__(kThreads)
+k_ruiz_err_inst(const int64_t* __restrict__ roff, const int64_t* __restrict__ coff, const double* __restrict__ row_inf,
+                const double* __restrict__ col_inf, double tol, int* __restrict__ inst_done, const SetupState* sst) {
+    if (sst->ruiz_done) return;
+    const int inst = blockIdx.x;
+    if (inst_done[inst]) return;
+    __shared__ double red[2 * 32];   // block_reduce needs 32 slots per reduced value
+    double e[2] = {0.0, 0.0};
+    for (int64_t i = roff[inst] + threadIdx.x; i < roff[inst + 1]; i += blockDim.x)
+        if (row_inf[i] > kZeroDrop) e[0] = fmax(e[0], fabs(1.0 - row_inf[i]));
+    for (int64_t j = coff[inst] + threadIdx.x; j < coff[inst + 1]; j += blockDim.x)
+        if (col_inf[j] > kZeroDrop) e[1] = fmax(e[1], fabs(1.0 - col_inf[j]));
+    block_reduce<OpMax, double, 2>(e, red);
+    if (threadIdx.x == 0 && e[0] <= tol && e[1] <= tol) inst_done[inst] = 1;
+}
+
+// k_scale_factors for a block-diagonal LP: factor 1 for the rows / columns of instances whose
+// Ruiz test has passed.
+__global__ void k_scale_factors_inst(int k_count, const double* __restrict__ norm, double* __restrict__ step,
+                                     double* __restrict__ scale, const int* __restrict__ inst,
+                                     const int* __restrict__ inst_done, const SetupState* sst) {
+    if (sst->ruiz_done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k_count) return;
+    if (inst_done[inst[i]]) { step[i] = 1.0; return; }
+    const double r = (norm[i] > kZeroDrop) ? __ddiv_rn(1.0, __dsqrt_rn(norm[i])) : 1.0;
+    step[i] = r;
+    scale[i] = __dmul_rn(scale[i], r);
+}
+
 // Pock-Chambolle (alpha = 1) norms: sum |a| per column / per row, in storage order.
 __global__ void k_col_abs_sum(int n, const int64_t* __restrict__ col_ptr, const double* __restrict__ v,
                               double* __restrict__ out) {
@@ -293,13 +326,32 @@ vajra_status prepare_scaled(const DeviceLp& lp, Prepared& p, const ScalingOpts& 
         k_expand_cols<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), col_of.get());
         note_launch(1);
         VJ_CUDA(cudaMemsetAsync(sst, 0, sizeof(SetupState), st));
+        const bool per_instance = o.instances > 0;
+        DeviceBuffer<int> inst_done;
+        if (per_instance) {
+            VJ_TRY(inst_done.alloc(static_cast<size_t>(o.instances)));
+            VJ_CUDA(cudaMemsetAsync(inst_done.get(), 0, sizeof(int) * o.instances, st));
+        }
         for (int it = 0; it < o.ruiz_iterations; ++it) {
             k_col_inf<<<grid_for(n), kThreads, 0, st>>>(n, lp.col_ptr.get(), p.csc_val.get(), col_norm.get(), sst);
             k_row_inf<<<grid_for(m), kThreads, 0, st>>>(m, p.csr_ptr.get(), p.perm.get(), p.csc_val.get(),
                                                         row_norm.get(), sst);
-            k_ruiz_err<<<1, 1, 0, st>>>(o.ruiz_tolerance, sst);
-            k_scale_factors<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(), sst, 1);
-            k_scale_factors<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(), sst, 1);
+            if (per_instance) {
+                // per-instance tests first; the global one after it only ends the passes early
+                // once every instance has passed (then every factor below would be 1)
+                k_ruiz_err_inst<<<o.instances, kThreads, 0, st>>>(o.roff, o.coff, row_norm.get(), col_norm.get(),
+                                                                   o.ruiz_tolerance, inst_done.get(), sst);
+                k_ruiz_err<<<1, 1, 0, st>>>(o.ruiz_tolerance, sst);
+                k_scale_factors_inst<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(),
+                                                                       o.row_inst, inst_done.get(), sst);
+                k_scale_factors_inst<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(),
+                                                                       o.col_inst, inst_done.get(), sst);
+                note_launch(1);
+            } else {
+                k_ruiz_err<<<1, 1, 0, st>>>(o.ruiz_tolerance, sst);
+                k_scale_factors<<<grid_for(m), kThreads, 0, st>>>(m, row_norm.get(), r_k.get(), p.row_scale.get(), sst, 1);
+                k_scale_factors<<<grid_for(n), kThreads, 0, st>>>(n, col_norm.get(), c_k.get(), p.col_scale.get(), sst, 1);
+            }
             k_scale_matrix<<<grid_stride_blocks(nnz), kThreads, 0, st>>>(nnz, col_of.get(), lp.row_idx.get(),
                                                                           p.csc_val.get(), r_k.get(), c_k.get(), sst, 1);
             VJ_LAUNCH_CHECK();
