@@ -136,3 +136,35 @@ def test_batch_iteration_limit_across_graph_launches(cuda, precision):
             assert b["iterations"] == limit
     if precision == "fp64":
         assert sum(r["status_name"] == "ITERATION_LIMIT" for r in lim) >= 1
+
+
+def rows_scaled(lp, seed, decades=3.0):
+    """The same LP with row i of A and of its bounds multiplied by 10^u, u ~ U[-decades, decades]
+    (same sparsity, same solution x; Ruiz needs several more passes to balance it)."""
+    rng = np.random.default_rng(seed)
+    d = 10.0 ** rng.uniform(-decades, decades, size=lp.num_rows)
+    q = W.LP(**{**lp.__dict__})
+    q.values = lp.values * d[lp.row_idx]
+    q.row_lower = np.where(lp.row_lower > -1e20, lp.row_lower * d, lp.row_lower)
+    q.row_upper = np.where(lp.row_upper < 1e20, lp.row_upper * d, lp.row_upper)
+    q.y_planted = None
+    return q
+
+
+def test_batch_scales_each_instance_as_alone(cuda):
+    """Each instance ends its Ruiz passes on its own stopping test.  Instance A is solved next to
+    B and next to C, where C is B with its rows scaled over six decades (same sparsity, so the
+    set-up picks the same SpMV shapes with autotuning off; C needs many more Ruiz passes than
+    B).  A's results must be bit-identical in both batches; with one stopping test over the
+    packed matrix, A would take C's extra passes in the second batch."""
+    a = W.random_planted(300, 800, 6, seed=71)
+    b = W.random_planted(400, 1000, 6, seed=72)
+    c = rows_scaled(b, seed=73)
+    kw = dict(precision=V.PREC_FP64, autotune=0, iteration_limit=20000)
+    with_b = V.solve_batch([a, b], **kw)
+    with_c = V.solve_batch([a, c], **kw)
+    assert with_b[0]["status_name"] == "OPTIMAL"
+    assert with_b[0]["iterations"] == with_c[0]["iterations"]
+    np.testing.assert_array_equal(with_b[0]["x"], with_c[0]["x"])
+    np.testing.assert_array_equal(with_b[0]["y"], with_c[0]["y"])
+    assert with_b[0]["spectral_norm_estimate"] == with_c[0]["spectral_norm_estimate"]
