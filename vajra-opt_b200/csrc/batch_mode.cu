@@ -822,15 +822,15 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     VJ_TRY(counters.alloc(1));
     VJ_CUDA(cudaMemsetAsync(counters.get(), 0, sizeof(BatchCounters), st));
     BatchCounters* hc = nullptr;
-    VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hc), sizeof(BatchCounters)));
+    hc = static_cast<BatchCounters*>(pinned_scratch(sizeof(BatchCounters)));
+    if (!hc) { set_error("page-locked host memory for the batch counters"); return VAJRA_ERR_OUT_OF_MEMORY; }
     std::memset(hc, 0, sizeof(BatchCounters));
     struct Guard {
-        BatchCounters* h; cudaGraph_t g[2] = {nullptr, nullptr}; cudaGraphExec_t e[2] = {nullptr, nullptr};
+        cudaGraph_t g[2] = {nullptr, nullptr}; cudaGraphExec_t e[2] = {nullptr, nullptr};
         ~Guard() {
             for (int k = 0; k < 2; ++k) { if (e[k]) cudaGraphExecDestroy(e[k]); if (g[k]) cudaGraphDestroy(g[k]); }
-            if (h) cudaFreeHost(h);
         }
-    } guard{hc};
+    } guard;
 
     BControl bc{};
     bc.tol = o.tolerance;

@@ -197,6 +197,23 @@ int sm_count() {
     return sms;
 }
 
+void* pinned_scratch(size_t bytes) {
+    struct Block { void* p = nullptr; size_t size = 0; };
+    thread_local Block b;   // never freed: see the declaration
+    if (b.size < bytes) {
+        const size_t want = bytes < 4096 ? 4096 : bytes;
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, want, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        if (b.p) cudaFreeHost(b.p);   // only when a larger record is asked for
+        b.p = p;
+        b.size = want;
+    }
+    return b.p;
+}
+
 bool pdl_enabled() {
     static const bool on = [] {
         const char* e = std::getenv("VAJRA_PDL");

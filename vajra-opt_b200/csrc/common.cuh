@@ -49,6 +49,14 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
     return static_cast<unsigned>(g);
 }
 
+// Page-locked host memory for the small state record a solve reads back after every chunk
+// (at least `bytes`, 16-byte aligned): one block per host thread, allocated on its first use
+// and kept for the life of the process.  Freeing page-locked memory (cudaFreeHost) took from
+// 5 ms to over a second a call on a shared machine, more than a small LP's whole solve, when
+// every solve allocated and freed its own.  A thread runs one solve at a time, and a solve
+// uses one record, so the block is never shared.  nullptr if the allocation fails.
+void* pinned_scratch(size_t bytes);
+
 // Programmatic dependent launch.  The SpMV kernels are launched with programmatic stream
 // serialization: the next kernel's CTAs may be scheduled while the previous kernel in the
 // stream is still draining, which hides most of the launch gap between the two SpMVs of an

@@ -891,8 +891,8 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
 
     HState* S = dstate.get();
     HState* hs = nullptr;
-    VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hs), sizeof(HState)));
-    struct PinnedFree { HState* p; ~PinnedFree() { if (p) cudaFreeHost(p); } } pin_guard{hs};
+    hs = static_cast<HState*>(pinned_scratch(sizeof(HState)));
+    if (!hs) { set_error("page-locked host memory for the solver state"); return VAJRA_ERR_OUT_OF_MEMORY; }
 
     ControlParams cp{};
     cp.tol = o.tolerance;

@@ -330,11 +330,12 @@ vajra_status run_reference(vajra_pdhg* h, vajra_result* r) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     RefState* hs = nullptr;
-    VJ_CUDA(cudaMallocHost(reinterpret_cast<void**>(&hs), sizeof(RefState)));
+    hs = static_cast<RefState*>(pinned_scratch(sizeof(RefState)));
+    if (!hs) { set_error("page-locked host memory for the solver state"); return VAJRA_ERR_OUT_OF_MEMORY; }
     struct Cleanup {
-        cudaGraph_t* g; cudaGraphExec_t* e; RefState* h;
-        ~Cleanup() { if (*e) cudaGraphExecDestroy(*e); if (*g) cudaGraphDestroy(*g); if (h) cudaFreeHost(h); }
-    } cleanup{&graph, &exec, hs};
+        cudaGraph_t* g; cudaGraphExec_t* e;
+        ~Cleanup() { if (*e) cudaGraphExecDestroy(*e); if (*g) cudaGraphDestroy(*g); }
+    } cleanup{&graph, &exec};
 
     const auto t_iter = Clock::now();
     int64_t done_iters = 0;
