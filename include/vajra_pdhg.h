@@ -273,11 +273,13 @@ vajra_status vajra_pdhg_solve(const vajra_lp* lp, const vajra_opts* opts, vajra_
  * device set-up and the solve from the resident copy; destroy frees it. */
 vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra_pdhg** handle);
 /* Batched form: `count` independent LPs solved together (VAJRA_ALGO_HALPERN), packed
- * block-diagonally into one device problem with per-instance step sizes, primal weights,
- * restarts and termination.  VAJRA_PREC_MIXED runs an FP32 pass first (FP32 values, iterates
- * and sums, FP64 checks), in which each instance either reaches the tolerance or -- at
+ * block-diagonally into one device problem with per-instance scaling (each instance's Ruiz
+ * passes end on its own stopping test, as if it were solved alone), step sizes, primal
+ * weights, restarts and termination.  VAJRA_PREC_MIXED runs an FP32 pass first (FP32 values,
+ * iterates and sums, FP64 checks), in which each instance either reaches the tolerance or -- at
  * mixed_switch_tolerance or on a stall -- hands over to an FP64 pass that restarts it from its
- * FP32 candidate; VAJRA_PREC_FP64 runs the FP64 pass alone.  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
+ * FP32 candidate; VAJRA_PREC_FP64 runs the FP64 pass alone.  time_limit is checked every 2048
+ * iterations.  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
  * the reference's benchmark Suite 2 issues them (apps/benchmark_runner.cpp:936-944).
  * results[i] receives instance i; every result's device_time_sec is the whole batch's. */
 vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const vajra_opts* opts,
