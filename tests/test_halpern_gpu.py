@@ -449,3 +449,57 @@ def test_chained_launch_changes_no_result(cuda, tmp_path):
         assert [r["iterations"], r["status"]] == plain[name + "_it"].tolist()
         np.testing.assert_array_equal(r["x"], plain[name + "_x"])
         np.testing.assert_array_equal(r["y"], plain[name + "_y"])
+
+
+def test_solves_after_a_device_reset(cuda, tmp_path):
+    """A caller that resets the device (cudaDeviceReset) between solves ends the context that
+    owned the library's cached device blocks and page-locked records.  The cache keys blocks by
+    the driver's context id and forgets those of an ended context, so the solves after the
+    reset allocate afresh and give the results of the solves before it.  Runs in a child
+    process (the reset would pull the device out from under this process's torch state); the
+    child first checks through the driver that the reset gave the device a new context id."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = r'''
+import ctypes, json, sys
+import numpy as np
+import vajra_pdhg as V
+from vajra_pdhg import workloads as W
+drv = ctypes.CDLL("libcuda.so.1")
+def ctx_id():
+    c = ctypes.c_void_p()
+    assert drv.cuCtxGetCurrent(ctypes.byref(c)) == 0 and c.value
+    i = ctypes.c_ulonglong()
+    assert drv.cuCtxGetId(c, ctypes.byref(i)) == 0
+    return i.value
+lp = W.random_planted(300, 800, 6, seed=5)
+before = V.solve(lp, precision=V.PREC_FP64)
+batch_before = V.solve_batch([lp, lp], precision=V.PREC_FP64, autotune=0)
+id0 = ctx_id()
+rt = ctypes.CDLL("libcudart.so.12")
+assert rt.cudaDeviceReset() == 0
+assert rt.cudaFree(None) == 0
+id1 = ctx_id()
+if id1 == id0:
+    print(json.dumps({"same_context": True}))
+    sys.exit(3)
+after = V.solve(lp, precision=V.PREC_FP64)
+batch_after = V.solve_batch([lp, lp], precision=V.PREC_FP64, autotune=0)
+out = {"status": [before["status_name"], after["status_name"]],
+       "iterations": [before["iterations"], after["iterations"]],
+       "x_equal": bool(np.array_equal(before["x"], after["x"])),
+       "batch": [r["status_name"] for r in batch_after],
+       "batch_x_equal": bool(np.array_equal(batch_before[0]["x"], batch_after[0]["x"]))}
+print(json.dumps(out))
+'''
+    env = dict(os.environ,
+               PYTHONPATH=os.pathsep.join([root, os.path.join(root, "vajra-opt_b200"), os.environ.get("PYTHONPATH", "")]))
+    p = subprocess.run([sys.executable, "-c", script], env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-3000:]
+    import json
+    out = json.loads(p.stdout.strip().splitlines()[-1])
+    assert out["status"] == ["OPTIMAL", "OPTIMAL"]
+    assert out["iterations"][0] == out["iterations"][1] and out["x_equal"]
+    assert out["batch"] == ["OPTIMAL", "OPTIMAL"] and out["batch_x_equal"]

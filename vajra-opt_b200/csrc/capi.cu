@@ -9,6 +9,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "solver.cuh"
@@ -49,9 +50,12 @@ struct CachedBlock {
     void* p;
     cudaEvent_t ready;
 };
+// (device, context id, size class)
+using BlockKey = std::tuple<int, unsigned long long, size_t>;
 struct BlockCache {
     std::mutex mu;
-    std::map<std::pair<int, size_t>, std::vector<CachedBlock>> free_blocks;
+    std::map<BlockKey, std::vector<CachedBlock>> free_blocks;
+    std::map<int, unsigned long long> device_ctx;   // the newest context seen per device
     size_t cached_bytes = 0;
 };
 BlockCache& block_cache() {
@@ -94,6 +98,56 @@ size_t block_cache_limit() {
     return limit;
 }
 
+unsigned long long current_context_id() {
+    // cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (CUDA 12.0 forms),
+    // so the library needs no link against the driver library
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    void* ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx) {
+        cudaFree(nullptr);   // makes the current device's primary context current
+        cudaGetLastError();
+        if (get_current(&ctx) != 0 || !ctx) return 0;
+    }
+    unsigned long long id = 0;
+    return get_id(ctx, &id) == 0 ? id : 0;
+}
+
+namespace {
+// Drops the cached blocks of `device` that belong to a context other than `ctx` (caller holds
+// the lock).  Only a reset replaces a device's context, and the reset freed those blocks and
+// ended their events, so they are forgotten, neither freed nor waited on.
+void forget_old_contexts(BlockCache& c, int device, unsigned long long ctx) {
+    auto seen = c.device_ctx.find(device);
+    if (seen != c.device_ctx.end() && seen->second == ctx) return;
+    c.device_ctx[device] = ctx;
+    for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
+        if (std::get<0>(it->first) == device && std::get<1>(it->first) != ctx) {
+            c.cached_bytes -= std::get<2>(it->first) * it->second.size();
+            it = c.free_blocks.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+}  // namespace
+
 // Frees every cached block of `device` (all devices for device < 0); returns the bytes freed.
 size_t release_cached_blocks(int device) {
     BlockCache& c = block_cache();
@@ -102,31 +156,39 @@ size_t release_cached_blocks(int device) {
     int cur = 0;
     const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
     for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
-        if (device >= 0 && it->first.first != device) { ++it; continue; }
-        cudaSetDevice(it->first.first);
-        for (const CachedBlock& b : it->second) {
-            if (b.ready) { cudaEventSynchronize(b.ready); cudaEventDestroy(b.ready); }
-            cudaFree(b.p);
-            freed += it->first.second;
-        }
-        c.cached_bytes -= it->first.second * it->second.size();
+        const int dev = std::get<0>(it->first);
+        const size_t cls = std::get<2>(it->first);
+        if (device >= 0 && dev != device) { ++it; continue; }
+        cudaSetDevice(dev);
+        if (std::get<1>(it->first) == current_context_id()) {
+            for (const CachedBlock& b : it->second) {
+                if (b.ready) { cudaEventSynchronize(b.ready); cudaEventDestroy(b.ready); }
+                cudaFree(b.p);
+                freed += cls;
+            }
+        }   // else: a context that a reset ended; its blocks are gone already
+        c.cached_bytes -= cls * it->second.size();
         it = c.free_blocks.erase(it);
     }
     if (have_cur) cudaSetDevice(cur);
     return freed;
 }
 
-cudaError_t cached_alloc(void** p, size_t bytes, int* device) {
+cudaError_t cached_alloc(void** p, size_t bytes, int* device, unsigned long long* ctx) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     *device = dev;
+    const unsigned long long id = current_context_id();
+    *ctx = id;
     const size_t cls = size_class(bytes);
+    if (id == 0) return cudaMalloc(p, cls);   // context unknown: no caching (see cached_release)
     CachedBlock b{nullptr, nullptr};
     {
         BlockCache& c = block_cache();
         std::lock_guard<std::mutex> lock(c.mu);
-        auto it = c.free_blocks.find({dev, cls});
+        forget_old_contexts(c, dev, id);
+        auto it = c.free_blocks.find(BlockKey{dev, id, cls});
         if (it != c.free_blocks.end() && !it->second.empty()) {
             b = it->second.back();
             it->second.pop_back();
@@ -145,11 +207,23 @@ cudaError_t cached_alloc(void** p, size_t bytes, int* device) {
     return cudaMalloc(p, cls);
 }
 
-void cached_release(void* p, size_t bytes, int device) {
+void cached_release(void* p, size_t bytes, int device, unsigned long long ctx) {
     const size_t cls = size_class(bytes);
     int cur = 0;
     if (cudaGetDevice(&cur) != cudaSuccess) return;
     if (cur != device) cudaSetDevice(device);
+    if (ctx == 0) {   // allocated while the context id could not be read: not cached
+        cudaFree(p);
+        cudaGetLastError();
+        if (cur != device) cudaSetDevice(cur);
+        return;
+    }
+    if (current_context_id() != ctx) {
+        // allocated in a context that a reset has ended: the block was freed with it, and its
+        // address may belong to a new allocation by now
+        if (cur != device) cudaSetDevice(cur);
+        return;
+    }
     // Nothing still queued on the device may touch the block once it is handed out again:
     // an event on the releasing solve's stream (all of a solve's kernels use it), else the
     // whole device.  Not inside a stream capture, where neither works: the block is freed.
@@ -170,8 +244,9 @@ void cached_release(void* p, size_t bytes, int device) {
     if (usable) {
         BlockCache& c = block_cache();
         std::lock_guard<std::mutex> lock(c.mu);
+        forget_old_contexts(c, device, ctx);
         if (c.cached_bytes + cls <= block_cache_limit()) {
-            c.free_blocks[{device, cls}].push_back(CachedBlock{p, ready});
+            c.free_blocks[BlockKey{device, ctx, cls}].push_back(CachedBlock{p, ready});
             c.cached_bytes += cls;
             kept = true;
         }
@@ -200,6 +275,15 @@ int sm_count() {
 void* pinned_scratch(size_t bytes) {
     struct Block { void* p = nullptr; size_t size = 0; };
     thread_local Block b;   // never freed: see the declaration
+    if (b.p) {
+        // A reset of the context that allocated it (cudaDeviceReset) releases the block: then
+        // the address is no longer page-locked host memory and a new block is taken.
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, b.p) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+            cudaGetLastError();
+            b = Block{};
+        }
+    }
     if (b.size < bytes) {
         const size_t want = bytes < 4096 ? 4096 : bytes;
         void* p = nullptr;

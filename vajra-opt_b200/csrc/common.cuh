@@ -54,7 +54,9 @@ inline unsigned grid_for(int64_t work, int threads = kThreads, int64_t cap = 1 <
 // and kept for the life of the process.  Freeing page-locked memory (cudaFreeHost) took from
 // 5 ms to over a second a call on a shared machine, more than a small LP's whole solve, when
 // every solve allocated and freed its own.  A thread runs one solve at a time, and a solve
-// uses one record, so the block is never shared.  nullptr if the allocation fails.
+// uses one record, so the block is never shared.  The block is checked before each use: after a
+// reset of the context that allocated it (cudaDeviceReset), a new one is taken.  nullptr if the
+// allocation fails.
 void* pinned_scratch(size_t bytes);
 
 // Programmatic dependent launch.  The SpMV kernels are launched with programmatic stream
@@ -93,16 +95,24 @@ inline void launch_chained(void (*kernel)(Params...), unsigned grid, unsigned bl
     (void)cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-// Device blocks go through a process-wide cache keyed by (device, size class): a released
-// block is handed out again only after the work queued before its release has finished (the
-// ordering cudaFree gives; see ReleaseStreamScope) and is kept for
-// the next request of its size class on that device, which then needs no driver call.  A
-// solve allocates and releases the same few dozen buffers every run; on shared machines those
-// driver calls were where the occasional multi-second host stalls of a solve showed up.  At
-// most block_cache_limit() bytes are kept; beyond that blocks are freed.  Cached blocks keep
-// their old contents (so does fresh cudaMalloc memory: nothing may assume zeros).
-cudaError_t cached_alloc(void** p, size_t bytes, int* device);
-void cached_release(void* p, size_t bytes, int device);
+// Device blocks go through a process-wide cache keyed by (device, context, size class): a
+// released block is handed out again only after the work queued before its release has
+// finished (the ordering cudaFree gives; see ReleaseStreamScope) and is kept for the next
+// request of its size class on that device, which then needs no driver call.  A solve
+// allocates and releases the same few dozen buffers every run; on shared machines those driver
+// calls were where the occasional multi-second host stalls of a solve showed up.  At most
+// block_cache_limit() bytes are kept; beyond that blocks are freed.  Cached blocks keep their
+// old contents (so does fresh cudaMalloc memory: nothing may assume zeros).
+//
+// The context is the driver's unique id of the device's current context (`ctx` below).  A
+// reset of the device (cudaDeviceReset) ends that context and frees every block it held: the
+// cache then drops, without freeing or reusing, every block of an older context of the device,
+// and a buffer released after the reset that was allocated before it is dropped as well (its
+// address may already belong to a new allocation).
+cudaError_t cached_alloc(void** p, size_t bytes, int* device, unsigned long long* ctx);
+void cached_release(void* p, size_t bytes, int device, unsigned long long ctx);
+// The driver's id of the calling thread's current context (0 if it cannot be read).
+unsigned long long current_context_id();
 // While alive, blocks the calling thread releases on `device` are ordered after the work
 // queued so far on `st` (the stream every kernel of the current solve runs on) by an event,
 // instead of by a device-wide synchronisation.
@@ -127,9 +137,12 @@ public:
     ~DeviceBuffer() { reset(); }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), dev_(o.dev_) { o.p_ = nullptr; o.n_ = 0; }
+    DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), dev_(o.dev_), ctx_(o.ctx_) {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
     DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
-        if (this != &o) { reset(); p_ = o.p_; n_ = o.n_; dev_ = o.dev_; o.p_ = nullptr; o.n_ = 0; }
+        if (this != &o) { reset(); p_ = o.p_; n_ = o.n_; dev_ = o.dev_; ctx_ = o.ctx_; o.p_ = nullptr; o.n_ = 0; }
         return *this;
     }
     // Every allocation carries kPad spare elements, so 128-bit vector loads of the last
@@ -139,14 +152,14 @@ public:
         reset();
         if (n == 0) n = 1;   // keep a valid pointer for empty extents
         void* p = nullptr;
-        cudaError_t e = cached_alloc(&p, (n + kPad) * sizeof(T), &dev_);
+        cudaError_t e = cached_alloc(&p, (n + kPad) * sizeof(T), &dev_, &ctx_);
         if (e != cudaSuccess) { p_ = nullptr; return cuda_status(e, "cudaMalloc", __FILE__, __LINE__); }
         p_ = static_cast<T*>(p);
         n_ = n;
         return VAJRA_OK;
     }
     void reset() noexcept {
-        if (p_) cached_release(p_, (n_ + kPad) * sizeof(T), dev_);
+        if (p_) cached_release(p_, (n_ + kPad) * sizeof(T), dev_, ctx_);
         p_ = nullptr;
         n_ = 0;
     }
@@ -157,6 +170,7 @@ private:
     T* p_ = nullptr;
     size_t n_ = 0;
     int dev_ = 0;
+    unsigned long long ctx_ = 0;   // the context the block was allocated in
 };
 
 // ---------------------------------------------------------------------------------------
