@@ -168,3 +168,19 @@ def test_batch_scales_each_instance_as_alone(cuda):
     np.testing.assert_array_equal(with_b[0]["x"], with_c[0]["x"])
     np.testing.assert_array_equal(with_b[0]["y"], with_c[0]["y"])
     assert with_b[0]["spectral_norm_estimate"] == with_c[0]["spectral_norm_estimate"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_time_limit(cuda, precision):
+    """The time limit is checked after every launch of a pass graph (up to 32 chunks of 64
+    iterations): with 1 ms, the call ends after its first launch; instances not finished by
+    then report TIME_LIMIT with finite points (in mixed precision, their FP32 candidates)."""
+    prec = V.PREC_FP64 if precision == "fp64" else V.PREC_MIXED
+    lps = small_batch(8, seed=12, m_lo=3000, m_hi=8000)
+    res = V.solve_batch(lps, precision=prec, time_limit=1e-3)
+    names = [r["status_name"] for r in res]
+    assert "TIME_LIMIT" in names, names
+    for r in res:
+        assert r["status_name"] in ("OPTIMAL", "TIME_LIMIT"), r["status_message"]
+        assert r["iterations"] <= 32 * 64
+        assert np.all(np.isfinite(r["x"])) and np.all(np.isfinite(r["y"]))
