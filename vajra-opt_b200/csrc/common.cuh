@@ -195,9 +195,11 @@ __device__ __forceinline__ T warp_reduce(T v) {
 }
 
 // Reduces NV values per thread across the block; the result is valid in thread 0.
-// `smem` must hold NV * 32 values.  All threads of the block must call it.
-template <class Op, typename T, int NV>
-__device__ __forceinline__ void block_reduce(T (&v)[NV], T* smem) {
+// `smem` holds 32 slots per value (checked at compile time).  All threads of the block must
+// call it.
+template <class Op, typename T, int NV, int S>
+__device__ __forceinline__ void block_reduce(T (&v)[NV], T (&smem)[S]) {
+    static_assert(S >= NV * 32, "block_reduce needs 32 shared slots per reduced value");
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int nwarps = (blockDim.x + 31) >> 5;

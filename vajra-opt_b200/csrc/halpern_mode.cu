@@ -41,7 +41,7 @@ constexpr double kGuardTol = 1e-7;   // tol::kPrimalFeasibility / kDualFeasibili
 __device__ __forceinline__ bool finite_lo(double l) { return l > -1e20; }
 __device__ __forceinline__ bool finite_up(double u) { return u < 1e20; }
 
-__device__ __forceinline__ void store_partials(double (&v)[kQ], double* red, double* part) {
+__device__ __forceinline__ void store_partials(double (&v)[kQ], double (&red)[kQ * 32], double* part) {
     block_reduce<OpSum, double, kNS>(*reinterpret_cast<double(*)[kNS]>(v), red);
     block_reduce<OpMax, double, kNM>(*reinterpret_cast<double(*)[kNM]>(v + kNS), red);
     if (threadIdx.x == 0)
