@@ -278,8 +278,9 @@ vajra_status vajra_pdhg_create(const vajra_lp* lp, const vajra_opts* opts, vajra
  * weights, restarts and termination.  VAJRA_PREC_MIXED runs an FP32 pass first (FP32 values,
  * iterates and sums, FP64 checks), in which each instance either reaches the tolerance or -- at
  * mixed_switch_tolerance or on a stall -- hands over to an FP64 pass that restarts it from its
- * FP32 candidate; VAJRA_PREC_FP64 runs the FP64 pass alone.  time_limit is checked every 2048
- * iterations.  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
+ * FP32 candidate; VAJRA_PREC_FP64 runs the FP64 pass alone.  Each pass runs on the device in
+ * graph launches of many chunks; time_limit is checked after each (the first launch of a pass
+ * runs 2048 iterations, later ones what fits in the time left at the measured rate).  Replaces a host loop of solve_pdhg_gpu calls (gpu.hpp:59), as
  * the reference's benchmark Suite 2 issues them (apps/benchmark_runner.cpp:936-944).
  * results[i] receives instance i; every result's device_time_sec is the whole batch's. */
 vajra_status vajra_pdhg_solve_batch(int32_t count, const vajra_lp* lps, const vajra_opts* opts,

@@ -108,9 +108,10 @@ def test_batch_mixed_iteration_limit_inside_the_fp32_pass(cuda):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_batch_iteration_limit_across_graph_launches(cuda, precision):
-    """A pass runs up to 32 chunks of 64 iterations per graph launch (a WHILE node repeats the
-    chunk on the device) and a last partial chunk directly.  A limit of 33 chunks + 17
-    iterations crosses a launch boundary and ends in a partial chunk.  Instances that finish
+    """The first graph launch of a pass runs 32 chunks of 64 iterations (a WHILE node repeats
+    the chunk on the device), later launches what is left up to the limit, and a last partial
+    chunk runs directly.  A limit of 33 chunks + 17 iterations crosses a launch boundary and
+    ends in a partial chunk.  Instances that finish
     in their first pass before it give the unlimited call's results (same status and count).  In the
     FP64-only form the others stop at exactly the limit; in mixed precision an instance's own
     count can be lower (the FP64 pass starts when the FP32 pass has ended for all)."""
@@ -172,9 +173,10 @@ def test_batch_scales_each_instance_as_alone(cuda):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_batch_time_limit(cuda, precision):
-    """The time limit is checked after every launch of a pass graph (up to 32 chunks of 64
-    iterations): with 1 ms, the call ends after its first launch; instances not finished by
-    then report TIME_LIMIT with finite points (in mixed precision, their FP32 candidates)."""
+    """The time limit is checked after every launch of a pass graph (the first one runs 32
+    chunks of 64 iterations, later ones what fits in the time left): with 1 ms, the call ends
+    after its first launch; instances not finished by then report TIME_LIMIT with finite
+    points (in mixed precision, their FP32 candidates)."""
     prec = V.PREC_FP64 if precision == "fp64" else V.PREC_MIXED
     lps = small_batch(8, seed=12, m_lo=3000, m_hi=8000)
     res = V.solve_batch(lps, precision=prec, time_limit=1e-3)

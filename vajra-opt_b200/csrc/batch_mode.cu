@@ -13,7 +13,7 @@
 // terms, one thread per instance runs the restart / primal-weight / termination logic
 // (same rules as the single-LP solver), and one thread counts the active instances.  A pass
 // is one CUDA graph whose WHILE node repeats the chunk (iterations plus check) on the device
-// while an instance is active, up to kChunksPerLaunch chunks a launch; the host reads the
+// while an instance is active, up to a chunk budget per launch; the host reads the
 // counters once per launch.  No kernel waits on another kernel, so nothing in this path can
 // spin, and the loop's chunk budget ends every launch.
 //
@@ -61,9 +61,12 @@ struct BatchCounters {
     long long chunks;
 };
 
-// Chunks one launch of a pass graph may run before the host looks at the counters again
-// (time limit, iteration limit): 2048 iterations at 64 per chunk.
-constexpr int kChunksPerLaunch = 32;
+// Chunks one launch of a pass graph may run before the host looks at the counters again.
+// The first launch of a pass runs kFirstLaunchChunks; later ones as many as the time left
+// allows at the chunk rate the host has measured (all of the pass, up to kMaxLaunchChunks,
+// without a time limit), so a pass without a time limit takes one or two launches.
+constexpr int kFirstLaunchChunks = 32;
+constexpr int kMaxLaunchChunks = 4096;
 
 __device__ __forceinline__ void instance_weights(const BatchArrays& S, int i) {
     const long long kb = S.k_base[i];
@@ -905,6 +908,8 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
     auto run_pass = [&](auto tag) -> vajra_status {
         using T = decltype(tag);
         const int k = sizeof(T) == 4 ? 0 : 1;
+        long long pass_chunks = 0;   // chunks this pass has run, and the host time they took
+        double pass_seconds = 0.0;
         while (launched < max_iter) {
             const int64_t remaining = max_iter - launched;
             if (remaining >= K) {
@@ -929,14 +934,25 @@ vajra_status run_batch(int count, const vajra_lp* lps, const vajra_opts& o, vajr
                     graph_kernels[k] = launch_count() - before;
                     launch_count() = before;
                 }
-                const int64_t budget = remaining / K < kChunksPerLaunch ? remaining / K : kChunksPerLaunch;
+                int64_t budget = kFirstLaunchChunks;
+                if (pass_chunks > 0) {
+                    // chunks that fit in the time left at this pass's measured rate (at least one)
+                    const double per_chunk = pass_seconds / static_cast<double>(pass_chunks);
+                    const double left_s = o.time_limit - seconds_since(t_start);
+                    const double fit = per_chunk > 0.0 ? left_s / per_chunk : static_cast<double>(kMaxLaunchChunks);
+                    budget = fit >= kMaxLaunchChunks ? kMaxLaunchChunks : (fit < 1.0 ? 1 : static_cast<int64_t>(fit));
+                }
+                if (remaining / K < budget) budget = remaining / K;
                 const long long chunks_before = hc->chunks;
+                const auto t_launch = Clock::now();
                 hc->left = static_cast<int>(budget);
                 VJ_CUDA(cudaMemcpyAsync(&counters.get()->left, &hc->left, sizeof(int), cudaMemcpyHostToDevice, st));
                 VJ_CUDA(cudaGraphLaunch(guard.e[k], st));
                 VJ_CUDA(cudaMemcpyAsync(hc, counters.get(), sizeof(BatchCounters), cudaMemcpyDeviceToHost, st));
                 VJ_CUDA(cudaStreamSynchronize(st));
                 const long long ran = hc->chunks - chunks_before;
+                pass_chunks += ran;
+                pass_seconds += seconds_since(t_launch);
                 note_launch(graph_kernels[k] * ran);
                 launched += ran * K;
                 if (o.verbose)
