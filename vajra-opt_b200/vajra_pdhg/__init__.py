@@ -62,9 +62,13 @@ def _result_dict(r: _capi.VajraResult, out: dict) -> dict:
     return d
 
 
-def _alloc(lp):
+def _alloc(lp, zeroed=True):
+    """Result arrays for one LP.  zeroed=False leaves them uninitialised: for calls that write
+    every element (the batched solver copies every instance's whole range before it returns
+    OK, and a failed call raises instead of returning them)."""
     m, n = int(lp.num_rows), int(lp.num_cols)
-    out = {"x": np.zeros(n), "row_value": np.zeros(m), "y": np.zeros(m), "d": np.zeros(n)}
+    new = np.zeros if zeroed else np.empty
+    out = {"x": new(n), "row_value": new(m), "y": new(m), "d": new(n)}
     r = _capi.VajraResult()
     r.col_value = _ptr(out["x"], _capi._dp)
     r.row_value = _ptr(out["row_value"], _capi._dp)
@@ -97,7 +101,7 @@ def solve_batch(lps, **opts) -> list:
     res = (_capi.VajraResult * len(lps))()
     outs = []
     for i, lp in enumerate(lps):
-        r, out = _alloc(lp)
+        r, out = _alloc(lp, zeroed=False)
         res[i] = r
         outs.append(out)
     o = default_opts(**opts)
