@@ -154,7 +154,8 @@ typedef struct vajra_opts {
     int32_t handover_mode;      /* MIXED: 0 = the FP64 phase restarts from the FP32 candidate
                                    (a new Halpern epoch anchored there); 1 = it continues the
                                    FP32 phase's epoch (iterate, anchor, counter and restart
-                                   references carried over)                                  */
+                                   references carried over); -1 (default) = 1 for LPs of 2^20
+                                   entries or more, else 0.  The batched solver restarts.     */
     double max_violation;       /* HALPERN: > 0 also requires, before OPTIMAL, the maxima that
                                    the engine's status guard checks (Solution::recompute_quality,
                                    src/engine/model.cpp:203-374) to be at most this on the

@@ -42,6 +42,7 @@ def test_default_opts():
     assert o.mixed_switch_tolerance == 2e-6 and o.mixed_reflection == 0.8 and o.reflection == 1.0
     assert o.degree_order == 0 and o.spmv_shape_a == 0 and o.spmv_shape_at == 0 and o.autotune == 1
     assert o.restart_sufficient == 0.2 and o.restart_necessary == 0.8 and o.restart_artificial == 0.36
+    assert o.handover_mode == -1   # by size: continue the FP32 epoch from 2^20 entries
     with pytest.raises(KeyError):
         V.default_opts(no_such_option=1)
 

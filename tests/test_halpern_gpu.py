@@ -503,3 +503,20 @@ print(json.dumps(out))
     assert out["status"] == ["OPTIMAL", "OPTIMAL"]
     assert out["iterations"][0] == out["iterations"][1] and out["x_equal"]
     assert out["batch"] == ["OPTIMAL", "OPTIMAL"] and out["batch_x_equal"]
+
+
+def test_handover_default_follows_the_lp_size(cuda):
+    """handover_mode = -1 (the default): below 2^20 entries the FP64 phase restarts from the
+    FP32 candidate (the same solve as handover_mode = 0), from 2^20 entries on it continues the
+    FP32 epoch (the same solve as handover_mode = 1)."""
+    small = W.random_planted(2000, 5000, 8, seed=24)
+    d, r = V.solve(small, precision=V.PREC_MIXED), V.solve(small, precision=V.PREC_MIXED, handover_mode=0)
+    assert d["iterations"] == r["iterations"] and d["fp64_iterations"] == r["fp64_iterations"]
+    np.testing.assert_array_equal(d["x"], r["x"])
+    big = W.random_large(200_000, 400_000, seed=5)
+    assert big.nnz >= 1 << 20
+    kw = dict(precision=V.PREC_MIXED, spmv_shape_a=-3, spmv_shape_at=-3)
+    d, c = V.solve(big, **kw), V.solve(big, handover_mode=1, **kw)
+    assert d["status_name"] == "OPTIMAL" and d["fp32_iterations"] > 0
+    assert d["iterations"] == c["iterations"] and d["fp64_iterations"] == c["fp64_iterations"]
+    np.testing.assert_array_equal(d["x"], c["x"])

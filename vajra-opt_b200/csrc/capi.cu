@@ -462,6 +462,7 @@ void vajra_default_opts(vajra_opts* o) {
     o->restart_artificial = 0.36;
     o->primal_weight_smoothing = 0.5;
     o->step_safety = 0.99;
+    o->handover_mode = -1;
 }
 
 // Static properties of `device`, read once per device (cudaGetDeviceProperties takes

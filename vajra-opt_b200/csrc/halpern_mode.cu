@@ -908,7 +908,12 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
     cp.metric = o.restart_metric == 1 ? 1 : 0;
     cp.max_violation = o.max_violation;
     cp.max_abs_violation = o.max_abs_violation;
-    cp.handover_mode = o.handover_mode == 1 ? 1 : 0;
+    // Hand-over to the FP64 phase: continue the FP32 phase's epoch on LPs of 2^20 entries or
+    // more (the degree-ordering threshold), restart from the FP32 candidate below it, unless
+    // the caller chose (1 / 0).  Measured: on four LPs of 3M-20M entries continuing was faster
+    // (1M x 2M: 5.09 -> 4.94 s) or the same; on LPs of 40k-400k entries it was slower.
+    const bool continue_epoch = o.handover_mode == 1 || (o.handover_mode < 0 && nnz >= kOrderMinNnz);
+    cp.handover_mode = continue_epoch ? 1 : 0;
     cp.stall_checks = o.mixed_stall_checks < 0 ? 0 : (o.mixed_stall_checks > kHist - 1 ? kHist - 1 : o.mixed_stall_checks);
     const int64_t max_iter = o.iteration_limit;
 
@@ -968,7 +973,7 @@ vajra_status run_halpern(vajra_pdhg* h, vajra_result* r) {
         }
         if (hs->stop) break;
         if (hs->phase != cur_phase) {
-            if (o.handover_mode == 1)
+            if (continue_epoch)
                 k_handover_keep<<<grid_for(mx), kThreads, 0, st>>>(m, n, p32.x.get(), p32.x0.get(), p32.xc.get(),
                                                                    p32.y.get(), p32.y0.get(), p32.yc.get(), p64.x.get(),
                                                                    p64.x0.get(), p64.xc.get(), p64.y.get(), p64.y0.get(),
