@@ -528,8 +528,8 @@ def run(args, world, rank, local, dist):
         per_iter = statistics.mean(x["per_iter_s"] for x in samples)
         setup = statistics.mean(x["setup_s"] for x in samples)
         # the iteration count the GPU arm's mixed solve needs on this LP (its line reports it as
-        # correct.iterations, 29,888 on the 1M x 2M LP, seed 1); both arms' CPU figures use it
-        iters_needed = int(os.environ.get("VAJRA_ITERS_TO_TOL", "29888"))
+        # correct.iterations, 29,056 on the 1M x 2M LP, seed 1); both arms' CPU figures use it
+        iters_needed = int(os.environ.get("VAJRA_ITERS_TO_TOL", "29056"))
         value = setup + per_iter * iters_needed
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(x["wall_s"] for x in samples),
